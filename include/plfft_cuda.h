@@ -1,0 +1,65 @@
+/*
+ * plfft_cuda.h -- device-side extensions of the plfft.h API for the B200
+ * implementation (libplfft_b200.so).  None of these has a counterpart in the
+ * reference's public header; each entry states the reference behaviour it
+ * extends.  Streams are passed as `void *` holding a cudaStream_t so that the
+ * header needs no CUDA include.
+ */
+#pragma once
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "plfft.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Arithmetic used by a plan's FP32 C2C stages (extension of
+ * plfft_config_set_data_type).  SPLIT_BF16 evaluates radix-16/32 DFT-matrix
+ * stages on tensor cores from bf16 hi/lo splits with FP32 accumulation. */
+typedef enum plfft_cuda_precision_t {
+  PLFFT_CUDA_PRECISION_FP32 = 0,
+  PLFFT_CUDA_PRECISION_SPLIT_BF16 = 1
+} plfft_cuda_precision_t;
+
+/* Multiply every output by `scale` (e.g. 1/n for a normalized round trip).
+ * Default 1.0: unnormalized, as the reference (docs/plfft.md:121-134).
+ * Fixed-point plans ignore it (they always scale by 1/n). */
+void plfft_cuda_config_set_scale(plfft_config_t *config, double scale);
+double plfft_cuda_config_get_scale(const plfft_config_t *config);
+
+void plfft_cuda_config_set_precision(plfft_config_t *config,
+                                     plfft_cuda_precision_t precision);
+plfft_cuda_precision_t
+plfft_cuda_config_get_precision(const plfft_config_t *config);
+
+/* Status of the calling thread's most recent execute (plfft_plan_execute has
+ * no return value, reference include/plfft.h:531). */
+plfft_status_t plfft_cuda_get_last_status(void);
+
+/* Bytes of device workspace a plan needs per concurrent execution. */
+plfft_status_t plfft_cuda_plan_get_workspace_size(const plfft_plan_t *plan,
+                                                  size_t *bytes);
+
+/* Number of kernel launches one execution issues. */
+int plfft_cuda_plan_get_launch_count(const plfft_plan_t *plan);
+
+/* Write a one-line description of the plan's device schedule (the analogue
+ * of the reference's plan_to_string, include/plfft/fft_plan.hpp:20-36). */
+plfft_status_t plfft_cuda_plan_describe(const plfft_plan_t *plan, char *buf,
+                                        size_t len);
+
+/* Stream-ordered execution on device pointers.  Returns once the work is
+ * enqueued.  `workspace` may be NULL: the plan's own workspace is used, in
+ * which case executions of the same plan on different streams must not
+ * overlap.  Pass a caller buffer of plfft_cuda_plan_get_workspace_size()
+ * bytes to run one plan concurrently on several streams. */
+plfft_status_t plfft_cuda_execute_async(const plfft_plan_t *plan,
+                                        const void *d_input, void *d_output,
+                                        void *d_workspace, void *stream);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,126 @@
+"""FP64 CPU oracle -- test infrastructure only.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg import this package, and only as the checker of the CUDA path.  It wraps
+``oracle/lib/liboracle.so`` (built from ``oracle/oracle.c`` by ``make -C
+oracle``), which restates the reference's transform definitions
+(arm/perf-libs-fft docs/plfft.md:100-212, include/plfft.h:98-134) as FP64
+direct sums and an FP64 mixed-radix FFT.
+
+Parity pins: the reference ships no golden vector files (its tests generate
+references analytically: test/delta_constant_test.hpp:38-63,
+test/pure_tone_test.hpp:36-62, test/simple_test.hpp:16-95,
+test/advanced_test_utils.hpp:49-124).  ``tests/test_oracle.py`` pins this
+oracle against those same analytic families and against
+``tests/golden/*.npz`` fixtures (see ``tests/golden/make_golden.py``).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "lib", "liboracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"oracle library missing: {path} (run make -C oracle)")
+        L = ctypes.CDLL(path)
+        i64 = ctypes.c_int64
+        dp = ctypes.c_void_p
+        for name in ("oracle_dft_c2c", "oracle_fft_c2c"):
+            f = getattr(L, name)
+            f.argtypes = [dp, dp, i64, i64, i64, i64, i64, i64, ctypes.c_int, ctypes.c_int]
+            f.restype = None
+        for name in ("oracle_r2c", "oracle_c2r", "oracle_r2r"):
+            f = getattr(L, name)
+            f.argtypes = [dp, dp, i64, i64, i64, i64, i64, i64, ctypes.c_int, ctypes.c_int]
+            f.restype = None
+        L.oracle_max_threads.restype = ctypes.c_int
+        _LIB = L
+    return _LIB
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def max_threads():
+    return lib().oracle_max_threads()
+
+
+def c2c(x, direction=-1, method="auto", threads=0):
+    """Batched C2C along the last axis; x complex (..., n). Returns complex128."""
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    n = x.shape[-1]
+    hm = int(np.prod(x.shape[:-1])) if x.ndim > 1 else 1
+    out = np.empty_like(x)
+    use_fft = method == "fft" or (method == "auto" and n > 4096)
+    f = lib().oracle_fft_c2c if use_fft else lib().oracle_dft_c2c
+    f(_ptr(x), _ptr(out), n, hm, 1, n, 1, n, int(direction), int(threads))
+    return out
+
+
+def r2c(x, method="auto", threads=0):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    n = x.shape[-1]
+    hm = int(np.prod(x.shape[:-1])) if x.ndim > 1 else 1
+    h = n // 2 + 1
+    out = np.empty(x.shape[:-1] + (h,), dtype=np.complex128)
+    use_fft = method == "fft" or (method == "auto" and n > 4096)
+    lib().oracle_r2c(_ptr(x), _ptr(out), n, hm, 1, n, 1, h, int(use_fft), int(threads))
+    return out
+
+
+def c2r(x, n, method="auto", threads=0):
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    h = n // 2 + 1
+    assert x.shape[-1] == h
+    hm = int(np.prod(x.shape[:-1])) if x.ndim > 1 else 1
+    out = np.empty(x.shape[:-1] + (n,), dtype=np.float64)
+    use_fft = method == "fft" or (method == "auto" and n > 4096)
+    lib().oracle_c2r(_ptr(x), _ptr(out), n, hm, 1, h, 1, n, int(use_fft), int(threads))
+    return out
+
+
+R2R_KINDS = {
+    "DCT_1": 0, "DCT_2": 1, "DCT_3": 2, "DCT_4": 3,
+    "DST_1": 4, "DST_2": 5, "DST_3": 6, "DST_4": 7,
+    "DHT": 8, "R2HC": 9, "HC2R": 10,
+}
+
+
+def r2r(x, kind, threads=0):
+    """kind: plfft_r2r_kind_t value or name (FFTW conventions)."""
+    k = R2R_KINDS[kind] if isinstance(kind, str) else int(kind)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    n = x.shape[-1]
+    hm = int(np.prod(x.shape[:-1])) if x.ndim > 1 else 1
+    out = np.empty_like(x)
+    lib().oracle_r2r(_ptr(x), _ptr(out), n, hm, 1, n, 1, n, k, int(threads))
+    return out
+
+
+def c2c_strided(buf_in, buf_out, n, howmany, istride, idist, ostride, odist, direction, method="dft"):
+    """C2C with explicit element strides on flat complex128 buffers (in place on buf_out)."""
+    assert buf_in.dtype == np.complex128 and buf_out.dtype == np.complex128
+    f = lib().oracle_fft_c2c if method == "fft" else lib().oracle_dft_c2c
+    f(_ptr(buf_in), _ptr(buf_out), n, howmany, istride, idist, ostride, odist, int(direction), 0)
+    return buf_out
+
+
+def rel_l2(got, ref):
+    got = np.asarray(got, dtype=np.complex128 if np.iscomplexobj(got) else np.float64)
+    ref = np.asarray(ref)
+    num = np.linalg.norm((got - ref).ravel())
+    den = np.linalg.norm(ref.ravel())
+    return float(num / den) if den > 0 else float(num)
+
+
+def fp32_tol(n):
+    """FP32 gate: rel-L2 <= 4 * log2(N) * 2^-24."""
+    return 4.0 * max(1.0, np.log2(max(n, 2))) * 2.0 ** -24

@@ -1,0 +1,386 @@
+// Planner: radix factorization, device twiddle tables and C2C schedules.
+#include "plan.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <sstream>
+
+namespace plfft_b200 {
+
+// ---------------------------------------------------------------------------
+// number theory helpers
+// ---------------------------------------------------------------------------
+bool is_prime(int64_t n) {
+  if (n < 2) return false;
+  for (int64_t d = 2; d * d <= n; ++d)
+    if (n % d == 0) return false;
+  return true;
+}
+
+bool is_smooth(int64_t n) {
+  if (n < 1) return false;
+  for (int p : {2, 3, 5, 7, 11, 13})
+    while (n % p == 0) n /= p;
+  return n == 1;
+}
+
+// Split n into radices <= max_radix, largest first.  Mirrors the intent of
+// the reference's factorize_descending (src/factorize.hpp:95-111): greedy
+// division by the largest available kernel size.  The radix menu here is the
+// set of on-chip codelets {16, 8, 4, 2, 13, 11, 7, 5, 3} (32 in the register
+// engine).
+std::vector<int> factor_radices(int64_t n, int max_radix) {
+  std::vector<int> r;
+  const int pow2_menu[] = {32, 16, 8, 4, 2};
+  for (int p : pow2_menu) {
+    if (p > max_radix) continue;
+    while (n % p == 0) {
+      r.push_back(p);
+      n /= p;
+    }
+  }
+  for (int p : {13, 11, 7, 5, 3}) {
+    while (n % p == 0) {
+      r.push_back(p);
+      n /= p;
+    }
+  }
+  if (n != 1) r.clear();
+  return r;
+}
+
+void unit_root(int64_t k, int64_t n, double& c, double& s) {
+  // cos/sin of 2 pi k / n with octant reduction in integers so that the
+  // argument handed to libm is small and exact symmetry points are exact
+  k %= n;
+  if (k < 0) k += n;
+  const long double kpi = 3.141592653589793238462643383279502884L;
+  __int128 k8 = (__int128)8 * k;
+  int64_t oct = int64_t(k8 / n);
+  int64_t rem = int64_t(k8 - (__int128)oct * n);
+  long double r = (long double)rem / (long double)n * (kpi / 4.0L);
+  long double c0, s0;
+  if (oct % 2 == 0) {
+    c0 = cosl(r);
+    s0 = sinl(r);
+  } else {
+    long double r2 = kpi / 4.0L - r;
+    c0 = cosl(r2);
+    s0 = -sinl(r2);
+    oct += 1;
+  }
+  int64_t q = (oct / 2) % 4;
+  long double cc = c0, ss = s0;
+  if (q == 1) { cc = -s0; ss = c0; }
+  if (q == 2) { cc = -c0; ss = -s0; }
+  if (q == 3) { cc = s0; ss = -c0; }
+  c = double(cc);
+  s = double(ss);
+}
+
+static float2 root_f(int64_t k, int64_t n, int sign) {
+  double c, s;
+  unit_root(k, n, c, s);
+  return make_float2(float(c), float(sign * s));
+}
+
+FftDesc make_desc(int n, const std::vector<int>& radices, std::vector<float2>& tw) {
+  FftDesc d{};
+  d.n = n;
+  d.nstages = int(radices.size());
+  int ns = 1;
+  for (size_t s = 0; s < radices.size(); ++s) {
+    const int R = radices[s];
+    Stage& st = d.st[s];
+    st.radix = R;
+    st.ns = ns;
+    st.ns_shift = (ns & (ns - 1)) == 0 ? __builtin_ctz(unsigned(ns)) : -1;
+    st.tw_off = int(tw.size());
+    if (ns > 1) {
+      // rows i = 1..R-1, entry r: exp(-2 pi i r i / (ns R))
+      for (int i = 1; i < R; ++i)
+        for (int r = 0; r < ns; ++r) tw.push_back(root_f(int64_t(r) * i, int64_t(ns) * R, -1));
+    }
+    ns *= R;
+  }
+  return d;
+}
+
+static int ilog2(int64_t n) {
+  int l = 0;
+  while ((int64_t(1) << l) < n) ++l;
+  return l;
+}
+static bool is_pow2(int64_t n) { return n > 0 && (n & (n - 1)) == 0; }
+
+// ---------------------------------------------------------------------------
+// register-engine C2C node
+// ---------------------------------------------------------------------------
+struct RegChoice {
+  int e = 0, t = 0, g = 0;
+  std::vector<int> radices;
+};
+
+static bool choose_reg(int64_t n, RegChoice& rc) {
+  if (!is_pow2(n) || n < 64 || n > kMaxOnChip) return false;
+  rc.e = n >= 1024 ? 32 : 16;
+  int64_t rest = n;
+  std::vector<int> big;
+  while (rest % rc.e == 0 && rest >= rc.e) {
+    big.push_back(rc.e);
+    rest /= rc.e;
+  }
+  rc.radices.clear();
+  if (rest > 1) rc.radices.push_back(int(rest));
+  rc.radices.insert(rc.radices.end(), big.begin(), big.end());
+  rc.t = int(n / rc.e);
+  rc.g = std::max(1, 256 / rc.t);
+  while (rc.g > 1 && reg_smem_bytes(int(n), rc.g) > 100 * 1024) rc.g /= 2;
+  return true;
+}
+
+struct C2CRegNode : Node {
+  RegLaunch base{};
+  int e = 0, dir = -1;
+  DevBuf tw;
+  std::vector<int> radices;
+  cudaError_t run(const void* in, void* out, void*, cudaStream_t st) const override {
+    RegLaunch L = base;
+    L.in = static_cast<const float2*>(in);
+    L.out = static_cast<float2*>(out);
+    return launch_c2c_reg(e, dir, L, st);
+  }
+  std::string describe() const override {
+    std::ostringstream o;
+    o << "(c2c-reg n=" << base.desc.n << " e=" << e << " t=" << base.t << " g=" << base.g
+      << " radices=";
+    for (size_t i = 0; i < radices.size(); ++i) o << (i ? "x" : "") << radices[i];
+    o << ")";
+    return o.str();
+  }
+};
+
+// ---------------------------------------------------------------------------
+// shared-memory tile C2C node (any smooth n <= kMaxOnChip, any strides)
+// ---------------------------------------------------------------------------
+static int tile_max_threads(int maxe) { return maxe <= 16 ? 512 : 256; }
+
+// threads needed so every stage fits the per-thread butterfly budget
+static int tile_threads(int n, const std::vector<int>& radices, int c, int maxe) {
+  int need = 32;
+  for (int R : radices) {
+    const int64_t bf = int64_t(c) * (n / R);
+    const int per = maxe / R;
+    need = std::max<int64_t>(need, (bf + per - 1) / per);
+  }
+  return (need + 31) / 32 * 32;
+}
+
+struct TileChoice {
+  int maxe = 16, c = 1, nthr = 32, ld = 1;
+  std::vector<int> radices;
+};
+
+static bool choose_tile(int64_t n, bool interleaved, TileChoice& tc) {
+  if (n > kMaxOnChip || !is_smooth(n)) return false;
+  tc.radices = factor_radices(n, 16);
+  tc.ld = spad_len(int(n));
+  for (int maxe : {16, 32}) {
+    tc.maxe = maxe;
+    int c = interleaved ? 16 : int(std::max<int64_t>(1, std::min<int64_t>(64, 4096 / n)));
+    while (c > 1 && (tile_smem_bytes(tc.ld, c) > 160 * 1024 ||
+                     tile_threads(int(n), tc.radices, c, maxe) > tile_max_threads(maxe)))
+      c /= 2;
+    if (tile_smem_bytes(tc.ld, c) <= 200 * 1024 &&
+        tile_threads(int(n), tc.radices, c, maxe) <= tile_max_threads(maxe)) {
+      tc.c = c;
+      tc.nthr = std::max(64, tile_threads(int(n), tc.radices, c, maxe));
+      return true;
+    }
+  }
+  return false;
+}
+
+struct C2CTileNode : Node {
+  TileLaunch base{};
+  int maxe = 16, dir = -1;
+  DevBuf tw;
+  std::vector<int> radices;
+  cudaError_t run(const void* in, void* out, void*, cudaStream_t st) const override {
+    TileLaunch L = base;
+    L.in = static_cast<const float2*>(in);
+    L.out = static_cast<float2*>(out);
+    return launch_c2c_tile(maxe, dir, L, st);
+  }
+  std::string describe() const override {
+    std::ostringstream o;
+    o << "(c2c-tile n=" << base.desc.n << " c=" << base.c << " threads=" << base.nthr
+      << " radices=";
+    for (size_t i = 0; i < radices.size(); ++i) o << (i ? "x" : "") << radices[i];
+    o << ")";
+    return o.str();
+  }
+};
+
+static std::unique_ptr<C2CTileNode> make_tile(int64_t n, int64_t ntr, const Addr& ia, const Addr& oa,
+                                              int dir, float scale, bool interleaved,
+                                              std::string* why) {
+  TileChoice tc;
+  if (!choose_tile(n, interleaved, tc)) {
+    if (why) *why = "no on-chip schedule for n=" + std::to_string(n);
+    return nullptr;
+  }
+  auto node = std::make_unique<C2CTileNode>();
+  std::vector<float2> tw;
+  node->base.desc = make_desc(int(n), tc.radices, tw);
+  if (node->tw.upload(tw) != cudaSuccess) {
+    if (why) *why = "device allocation failed";
+    return nullptr;
+  }
+  node->base.tw = node->tw.as<float2>();
+  node->base.ntr = ntr;
+  node->base.ia = ia;
+  node->base.oa = oa;
+  node->base.c = tc.c;
+  node->base.nthr = tc.nthr;
+  node->base.ld = tc.ld;
+  node->base.scale = scale;
+  node->base.post = TwoLevel{nullptr, nullptr, 0, 1};
+  node->maxe = tc.maxe;
+  node->dir = dir;
+  node->radices = tc.radices;
+  return node;
+}
+
+// ---------------------------------------------------------------------------
+// four-step C2C node: n = n1 * n2, both on chip
+//   pass 1: length-n1 column transforms over stride n2, times W_n^{n2 k1},
+//           into scratch Y[k1][n2]
+//   pass 2: length-n2 row transforms of Y, stored transposed to X[k1 + n1 k2]
+// The batch is processed in chunks so the scratch stays near L2 size.
+// ---------------------------------------------------------------------------
+struct C2CFourStepNode : Node {
+  int64_t n = 0, n1 = 0, n2 = 0;
+  Layout lay{};
+  int64_t chunk = 1;
+  std::unique_ptr<C2CTileNode> p1, p2;
+  DevBuf lo, hi;
+  size_t workspace() const override { return size_t(chunk) * size_t(n) * sizeof(float2); }
+  int launches() const override { return int(2 * ((lay.howmany + chunk - 1) / chunk)); }
+  cudaError_t run(const void* in, void* out, void* ws, cudaStream_t st) const override {
+    const float2* x = static_cast<const float2*>(in);
+    float2* y = static_cast<float2*>(out);
+    float2* s = static_cast<float2*>(ws);
+    for (int64_t m0 = 0; m0 < lay.howmany; m0 += chunk) {
+      const int64_t cnt = std::min(chunk, lay.howmany - m0);
+      TileLaunch a = p1->base;
+      a.in = x + m0 * lay.idist;
+      a.out = s;
+      a.ntr = cnt * n2;
+      cudaError_t e = launch_c2c_tile(p1->maxe, p1->dir, a, st);
+      if (e != cudaSuccess) return e;
+      TileLaunch b = p2->base;
+      b.in = s;
+      b.out = y + m0 * lay.odist;
+      b.ntr = cnt * n1;
+      e = launch_c2c_tile(p2->maxe, p2->dir, b, st);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+  std::string describe() const override {
+    std::ostringstream o;
+    o << "(c2c-four-step n=" << n << " " << n1 << "x" << n2 << " chunk=" << chunk << " "
+      << p1->describe() << " " << p2->describe() << ")";
+    return o.str();
+  }
+};
+
+static std::unique_ptr<Node> make_four_step(int64_t n, const Layout& lay, int dir, float scale,
+                                            std::string* why) {
+  // pick n1 <= n2, both smooth and on chip, n1 as close to sqrt(n) as possible
+  int64_t best = 0;
+  for (int64_t d = 2; d * d <= n; ++d) {
+    if (n % d) continue;
+    const int64_t e = n / d;
+    if (d <= kMaxOnChip && e <= kMaxOnChip && is_smooth(d) && is_smooth(e)) best = d;
+  }
+  if (!best) {
+    if (why) *why = "length " + std::to_string(n) + " has no on-chip four-step split";
+    return nullptr;
+  }
+  auto node = std::make_unique<C2CFourStepNode>();
+  node->n = n;
+  node->n1 = best;
+  node->n2 = n / best;
+  node->lay = lay;
+  const int64_t target = 48ll << 20;  // scratch bytes per chunk
+  node->chunk = std::max<int64_t>(1, std::min<int64_t>(lay.howmany, target / (n * 8)));
+  const int64_t n1 = node->n1, n2 = node->n2;
+  // pass 1: transforms g = (member, column n2), element k = n1 index
+  Addr ia1{lay.idist, lay.istride, n2 * lay.istride, n2};
+  Addr oa1{n, 1, n2, n2};
+  node->p1 = make_tile(n1, 0, ia1, oa1, dir, 1.0f, true, why);
+  // pass 2: transforms g = (member, row k1), element k = n2 index
+  Addr ia2{n, n2, 1, n1};
+  Addr oa2{lay.odist, lay.ostride, n1 * lay.ostride, n1};
+  node->p2 = make_tile(n2, 0, ia2, oa2, dir, scale, false, why);
+  if (!node->p1 || !node->p2) return nullptr;
+  // two-level twiddle tables for W_n^e, e < n: lo[e % L] * hi[e / L]
+  int64_t L = int64_t(1) << ((ilog2(n) + 1) / 2);
+  std::vector<float2> lo(L), hi((n + L - 1) / L);
+  for (int64_t i = 0; i < L; ++i) lo[i] = root_f(i, n, -1);
+  for (size_t i = 0; i < hi.size(); ++i) hi[i] = root_f(int64_t(i) * L, n, -1);
+  if (node->lo.upload(lo) != cudaSuccess || node->hi.upload(hi) != cudaSuccess) {
+    if (why) *why = "device allocation failed";
+    return nullptr;
+  }
+  node->p1->base.post = TwoLevel{node->lo.as<float2>(), node->hi.as<float2>(), n, int(L)};
+  return node;
+}
+
+std::unique_ptr<Node> make_c2c_node(int64_t n, const Layout& lay, int dir, float scale,
+                                    int precision, std::string* why) {
+  (void)precision;
+  const bool unit = lay.istride == 1 && lay.ostride == 1;
+  const bool interleaved = !unit && (lay.howmany > 1) &&
+                           (std::llabs(lay.idist) < lay.istride || std::llabs(lay.odist) < lay.ostride);
+  RegChoice rc;
+  if (unit && choose_reg(n, rc)) {
+    auto node = std::make_unique<C2CRegNode>();
+    std::vector<float2> tw;
+    node->base.desc = make_desc(int(n), rc.radices, tw);
+    if (node->tw.upload(tw) != cudaSuccess) {
+      if (why) *why = "device allocation failed";
+      return nullptr;
+    }
+    node->base.tw = node->tw.as<float2>();
+    node->base.howmany = lay.howmany;
+    node->base.istride = lay.istride;
+    node->base.idist = lay.idist;
+    node->base.ostride = lay.ostride;
+    node->base.odist = lay.odist;
+    node->base.t = rc.t;
+    node->base.g = rc.g;
+    node->base.scale = scale;
+    node->e = rc.e;
+    node->dir = dir;
+    node->radices = rc.radices;
+    return node;
+  }
+  if (n <= kMaxOnChip && is_smooth(n)) {
+    Addr ia{lay.idist, 0, lay.istride, 1};
+    Addr oa{lay.odist, 0, lay.ostride, 1};
+    return make_tile(n, lay.howmany, ia, oa, dir, scale, interleaved, why);
+  }
+  if (is_smooth(n)) return make_four_step(n, lay, dir, scale, why);
+  if (why) *why = "length " + std::to_string(n) + " needs a convolution schedule";
+  return nullptr;
+}
+
+PlanData::~PlanData() {
+  if (stream) cudaStreamDestroy(stream);
+}
+
+}  // namespace plfft_b200

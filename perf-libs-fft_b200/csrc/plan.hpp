@@ -1,0 +1,128 @@
+// Host-side planner and plan objects.
+//
+// The reference builds a tree of CPU plans (planner strategies in
+// src/planner/planner.cpp:49-182, legacy compositor in
+// src/compositor.cpp:57-316, level data in src/make_level_data.hpp:100-165)
+// and executes it level by level on host memory.  Here the planner picks a
+// schedule of device kernels instead: a single on-chip pass when the whole
+// transform fits in one CTA's shared memory, a four-step pair of passes for
+// longer smooth lengths, and Rader / Bluestein convolutions for lengths with
+// large prime factors.  Every node owns its device tables (twiddles, chirps,
+// permutations, convolution spectra) and runs asynchronously on a stream.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/plfft.h"
+#include "kernels.h"
+
+namespace plfft_b200 {
+
+enum class TKind { C2C = 0, R2C = 1, C2R = 2, R2R = 3 };
+
+// the configuration object behind plfft_config_t
+struct ConfigData {
+  int64_t n = 0;
+  int64_t howmany = 1;
+  int64_t istride = 1, idist = 0, ostride = 1, odist = 0;
+  TKind kind = TKind::C2C;
+  int payload = 0;  // direction for C2C, r2r kind for R2R
+  plfft_data_type_t data_type = PLFFT_DATA_TYPE_FP32;
+  plfft_io_alias_t alias = PLFFT_IO_NO_ALIAS;
+  plfft_sme_mode_t sme = PLFFT_SME_DISABLED;
+  plfft_rigor_t rigor = PLFFT_MEASURE;
+  // extensions
+  double scale = 1.0;
+  int precision = 0;  // 0 plain FP32, 1 split-BF16 tensor-core stages
+};
+
+// RAII device allocation
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  cudaError_t alloc(size_t b) {
+    release();
+    if (b == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e == cudaSuccess) bytes = b;
+    return e;
+  }
+  template <class T>
+  cudaError_t upload(const std::vector<T>& v) {
+    cudaError_t e = alloc(v.size() * sizeof(T));
+    if (e != cudaSuccess || v.empty()) return e;
+    return cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+// Strided batch layout, in elements of the buffer's own type.
+struct Layout {
+  int64_t howmany;
+  int64_t istride, idist, ostride, odist;
+};
+
+// One executable piece of a plan.
+struct Node {
+  virtual ~Node() = default;
+  // bytes of device workspace this node needs per execution
+  virtual size_t workspace() const { return 0; }
+  virtual cudaError_t run(const void* in, void* out, void* ws, cudaStream_t st) const = 0;
+  virtual std::string describe() const = 0;
+  // number of kernel launches per run (for launch accounting)
+  virtual int launches() const { return 1; }
+};
+
+// ---------------------------------------------------------------------------
+// factorization and stage tables
+// ---------------------------------------------------------------------------
+bool is_smooth(int64_t n);  // all prime factors in {2,3,5,7,11,13}
+bool is_prime(int64_t n);
+std::vector<int> factor_radices(int64_t n, int max_radix);
+// builds the stage list and appends the stage twiddle rows to tw
+FftDesc make_desc(int n, const std::vector<int>& radices, std::vector<float2>& tw);
+// exp(sign * 2 pi i k / n) in double
+void unit_root(int64_t k, int64_t n, double& c, double& s);
+
+// largest length one CTA transforms on chip
+constexpr int kMaxOnChip = 16384;
+
+// C2C FP32 node for a strided batch (dir -1/+1); scale applied on output.
+std::unique_ptr<Node> make_c2c_node(int64_t n, const Layout& lay, int dir, float scale,
+                                    int precision, std::string* why);
+
+// The plan object behind plfft_plan_t.
+struct PlanData {
+  ConfigData cfg;
+  std::unique_ptr<Node> root;
+  int device = 0;
+  DevBuf ws;  // workspace for plfft_plan_execute and *_async without a
+              // caller-provided workspace
+  // host-pointer staging (plfft_plan_execute with host buffers)
+  mutable std::mutex mu;
+  mutable DevBuf stage_in, stage_out;
+  cudaStream_t stream = nullptr;
+  int64_t in_elems = 0, out_elems = 0;  // span of one execute, elements
+  int in_bytes = 0, out_bytes = 0;      // element sizes
+  bool out_dense = false;               // the output span is fully written
+  ~PlanData();
+};
+
+}  // namespace plfft_b200

@@ -1,0 +1,126 @@
+// Plan construction per (kind, data type) and synchronous execution.
+//
+// Dispatch mirrors reference src/plfft.cpp:488-513 (dtype x kind) and
+// src/arm_fft1d_impl.hpp:109-147 (R2R wrapper, n == 1 copy); buffer spans
+// follow docs/plfft.md:100-166.
+#include "plan_kinds.hpp"
+
+#include <cstring>
+
+namespace plfft_b200 {
+
+static int scalar_bytes(plfft_data_type_t t) {
+  switch (t) {
+    case PLFFT_DATA_TYPE_FP32: return 4;
+    case PLFFT_DATA_TYPE_FP64: return 8;
+    case PLFFT_DATA_TYPE_FP16: return 2;
+    case PLFFT_DATA_TYPE_Q7: return 1;
+    case PLFFT_DATA_TYPE_Q15: return 2;
+  }
+  return 0;
+}
+
+// logical element counts of one transform (docs/plfft.md:109-116)
+static void io_counts(const ConfigData& c, int64_t& nin, int64_t& nout, bool& in_cplx, bool& out_cplx) {
+  const int64_t h = c.n / 2 + 1;
+  switch (c.kind) {
+    case TKind::C2C: nin = c.n; nout = c.n; in_cplx = out_cplx = true; break;
+    case TKind::R2C: nin = c.n; nout = h; in_cplx = false; out_cplx = true; break;
+    case TKind::C2R: nin = h; nout = c.n; in_cplx = true; out_cplx = false; break;
+    case TKind::R2R: nin = c.n; nout = c.n; in_cplx = out_cplx = false; break;
+  }
+}
+
+static int64_t span(int64_t howmany, int64_t dist, int64_t n, int64_t stride) {
+  return (howmany - 1) * (howmany > 1 ? dist : 0) + (n - 1) * stride + 1;
+}
+
+plfft_status_t build_plan(PlanData& p, std::string* why) {
+  const ConfigData& c = p.cfg;
+  cudaGetDevice(&p.device);
+  Layout lay{c.howmany, c.istride, c.howmany > 1 ? c.idist : 0, c.ostride, c.howmany > 1 ? c.odist : 0};
+  const float scale = float(c.scale);
+
+  if (c.data_type == PLFFT_DATA_TYPE_FP32) {
+    switch (c.kind) {
+      case TKind::C2C:
+        p.root = make_c2c_node(c.n, lay, c.payload, scale, c.precision, why);
+        break;
+      default:
+        if (why) *why = "transform kind not built yet";
+        break;
+    }
+  } else {
+    if (why) *why = "data type not supported on the device path";
+  }
+  if (!p.root) return PLFFT_PLAN_CREATION_FAILED;
+
+  int64_t nin = 0, nout = 0;
+  bool ic = false, oc = false;
+  io_counts(c, nin, nout, ic, oc);
+  const int sb = scalar_bytes(c.data_type);
+  p.in_bytes = sb * (ic ? 2 : 1);
+  p.out_bytes = sb * (oc ? 2 : 1);
+  p.in_elems = span(c.howmany, c.idist, nin, c.istride);
+  p.out_elems = span(c.howmany, c.odist, nout, c.ostride);
+  p.out_dense = (c.howmany == 1 && c.ostride == 1) ||
+                (c.ostride == 1 && c.odist == nout) ||
+                (c.odist == 1 && c.ostride == c.howmany);
+
+  if (p.ws.alloc(p.root->workspace()) != cudaSuccess) {
+    if (why) *why = "workspace allocation failed";
+    return PLFFT_PLAN_CREATION_FAILED;
+  }
+  if (cudaStreamCreate(&p.stream) != cudaSuccess) {
+    if (why) *why = "stream creation failed";
+    return PLFFT_PLAN_CREATION_FAILED;
+  }
+  return PLFFT_OK;
+}
+
+static bool on_device(const void* ptr) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+    cudaGetLastError();  // clear the sticky-free error of an unknown pointer
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+static cudaError_t ensure(DevBuf& b, size_t bytes) {
+  if (b.bytes >= bytes) return cudaSuccess;
+  return b.alloc(bytes);
+}
+
+plfft_status_t execute_sync(const PlanData& p, const void* in, void* out) {
+  std::lock_guard<std::mutex> lock(p.mu);
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != p.device) cudaSetDevice(p.device);
+  cudaError_t e = cudaSuccess;
+  const bool din = on_device(in), dout = on_device(out);
+  const size_t ibytes = size_t(p.in_elems) * p.in_bytes;
+  const size_t obytes = size_t(p.out_elems) * p.out_bytes;
+  const void* kin = in;
+  void* kout = out;
+  if (!din) {
+    e = ensure(p.stage_in, ibytes);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(p.stage_in.p, in, ibytes, cudaMemcpyHostToDevice, p.stream);
+    kin = p.stage_in.p;
+  }
+  if (e == cudaSuccess && !dout) {
+    e = ensure(p.stage_out, obytes);
+    // keep the bytes between strided outputs intact
+    if (e == cudaSuccess && !p.out_dense)
+      e = cudaMemcpyAsync(p.stage_out.p, out, obytes, cudaMemcpyHostToDevice, p.stream);
+    kout = p.stage_out.p;
+  }
+  if (e == cudaSuccess) e = p.root->run(kin, kout, p.ws.p, p.stream);
+  if (e == cudaSuccess && !dout) e = cudaMemcpyAsync(out, p.stage_out.p, obytes, cudaMemcpyDeviceToHost, p.stream);
+  const cudaError_t s = cudaStreamSynchronize(p.stream);
+  if (e == cudaSuccess) e = s;
+  if (cur != p.device) cudaSetDevice(cur);
+  return e == cudaSuccess ? PLFFT_OK : PLFFT_CUDA_ERROR;
+}
+
+}  // namespace plfft_b200

@@ -1,0 +1,65 @@
+"""Shared helpers for the parity tests (device buffers via torch, oracle checks)."""
+import numpy as np
+
+import oracle
+import plfft
+
+
+def span(howmany, dist, n, stride):
+    return (howmany - 1) * (dist if howmany > 1 else 0) + (n - 1) * stride + 1
+
+
+def seeded_complex(count, seed, scale=1.0):
+    rng = np.random.default_rng(seed)
+    re = rng.uniform(-1, 1, count)
+    im = rng.uniform(-1, 1, count)
+    return ((re + 1j * im) * scale).astype(np.complex64)
+
+
+def seeded_real(count, seed):
+    rng = np.random.default_rng(seed)
+    return rng.uniform(-1, 1, count).astype(np.float32)
+
+
+def to_dev(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def from_dev(t):
+    return t.cpu().numpy()
+
+
+def gather(buf, howmany, dist, n, stride):
+    """Logical (howmany, n) view of a strided flat buffer."""
+    idx = np.arange(howmany)[:, None] * dist + np.arange(n)[None, :] * stride
+    return buf[idx]
+
+
+def c2c_case(n, howmany=1, istride=1, idist=None, ostride=1, odist=None, direction=-1, seed=0,
+             alias=False, scale=1.0, host=False, method="auto"):
+    """Run a C2C plan on seeded data; return (got, ref) logical arrays."""
+    import torch
+
+    idist = n if idist is None else idist
+    odist = n if odist is None else odist
+    nin = span(howmany, idist, n, istride)
+    nout = span(howmany, odist, n, ostride)
+    x = seeded_complex(nin, seed)
+    xin = x.copy()
+    plan = plfft.make_plan("c2c", n, howmany, istride, idist, ostride, odist, direction=direction,
+                           alias=plfft.IoAlias.MAY_ALIAS if alias else plfft.IoAlias.NO_ALIAS, scale=scale)
+    if host:
+        out = np.zeros(nout, np.complex64) if not alias else x
+        plan.execute(x.ctypes.data, out.ctypes.data)
+        got_buf = out
+    else:
+        d_in = to_dev(x)
+        d_out = d_in if alias else torch.zeros(nout, dtype=torch.complex64, device="cuda")
+        plan.execute(d_in.data_ptr(), d_out.data_ptr())
+        got_buf = from_dev(d_out)
+    xl = gather(xin, howmany, idist, n, istride)
+    ref = oracle.c2c(xl.astype(np.complex128), direction, method=method) * scale
+    got = gather(got_buf, howmany, odist, n, ostride)
+    return got, ref, plan

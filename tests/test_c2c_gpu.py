@@ -1,0 +1,118 @@
+"""C2C FP32 parity: CUDA path (through the C-ABI) vs the FP64 oracle.
+
+Gate: rel-L2 <= 4*log2(N)*2^-24 per case (FP32 tolerance of the spec).
+Cases include the reference's own C2C list (test/c2c_f32.cpp:10-27).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from helpers import c2c_case
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [1, 2, 3, 4, 5, 7, 8, 9, 11, 12, 13, 15, 16, 25, 32, 49, 64, 100, 128, 143, 256, 360, 512,
+         1000, 1024, 2048, 2187, 4096, 8192, 16384]
+
+
+@pytest.mark.parametrize("n", SIZES)
+@pytest.mark.parametrize("direction", [-1, 1])
+def test_c2c_sizes(n, direction):
+    howmany = max(1, min(64, 65536 // n))
+    got, ref, plan = c2c_case(n, howmany, direction=direction, seed=n)
+    err = oracle.rel_l2(got, ref)
+    assert err <= oracle.fp32_tol(n), (n, err, plan.describe())
+
+
+# reference test/c2c_f32.cpp:10-27 (those with on-chip smooth lengths)
+REF_CASES = [
+    (2, 1, 1, 2, 1, 2), (8, 1, 1, 8, 1, 8), (16, 4, 1, 16, 1, 16), (8, 3, 2, 20, 2, 20),
+    (64, 2, 8, 600, 8, 600), (24, 4, 1, 32, 1, 32), (512, 1, 1, 512, 1, 512), (512, 3, 1, 512, 1, 512),
+    (512, 3, 3, 1, 3, 1), (1024, 4, 1, 1024, 1, 1024), (1024, 4, 1, 1024, 1024, 1),
+]
+
+
+@pytest.mark.parametrize("case", REF_CASES)
+@pytest.mark.parametrize("direction", [-1, 1])
+def test_c2c_reference_layouts(case, direction):
+    n, hm, is_, id_, os_, od = case
+    got, ref, plan = c2c_case(n, hm, is_, id_, os_, od, direction=direction, seed=7)
+    assert oracle.rel_l2(got, ref) <= oracle.fp32_tol(n), plan.describe()
+
+
+@pytest.mark.parametrize("n", [32768, 65536, 1 << 18, 1 << 20])
+def test_c2c_four_step(n):
+    howmany = 2
+    got, ref, plan = c2c_case(n, howmany, seed=3, method="fft")
+    assert "four-step" in plan.describe()
+    assert oracle.rel_l2(got, ref) <= oracle.fp32_tol(n), plan.describe()
+
+
+@pytest.mark.parametrize("n", [16, 1024, 1000, 4096])
+def test_c2c_in_place(n):
+    got, ref, _ = c2c_case(n, 8, alias=True, seed=11)
+    assert oracle.rel_l2(got, ref) <= oracle.fp32_tol(n)
+
+
+@pytest.mark.parametrize("n", [1024, 77 * 13])
+def test_c2c_host_pointers(n):
+    got, ref, _ = c2c_case(n, 5, host=True, seed=5)
+    assert oracle.rel_l2(got, ref) <= oracle.fp32_tol(n)
+
+
+def test_c2c_scale_round_trip():
+    import plfft
+    import torch
+
+    n, hm = 4096, 16
+    rng = np.random.default_rng(1)
+    x = (rng.uniform(-1, 1, n * hm) + 1j * rng.uniform(-1, 1, n * hm)).astype(np.complex64)
+    fwd = plfft.make_plan("c2c", n, hm, direction=-1)
+    bwd = plfft.make_plan("c2c", n, hm, direction=1, scale=1.0 / n)
+    d = torch.from_numpy(x).cuda()
+    y = torch.empty_like(d)
+    z = torch.empty_like(d)
+    fwd.execute(d.data_ptr(), y.data_ptr())
+    bwd.execute(y.data_ptr(), z.data_ptr())
+    assert oracle.rel_l2(z.cpu().numpy(), x) <= oracle.fp32_tol(n)
+
+
+def test_c2c_known_pairs():
+    """delta -> constant and pure tone (reference test/delta_constant_test.hpp:38-63,
+    test/pure_tone_test.hpp:36-62)."""
+    import plfft
+    import torch
+
+    n = 1024
+    plan = plfft.make_plan("c2c", n, 2, direction=-1)
+    x = np.zeros(2 * n, np.complex64)
+    x[0] = 1.0
+    k0 = 37
+    x[n + k0] = 1.0
+    d = torch.from_numpy(x).cuda()
+    y = torch.empty_like(d)
+    plan.execute(d.data_ptr(), y.data_ptr())
+    y = y.cpu().numpy()
+    assert np.allclose(y[:n], 1.0, atol=1e-6)
+    k = np.arange(n)
+    tone = np.exp(-2j * np.pi * k * k0 / n)
+    assert np.abs(y[n:] - tone).max() < 1e-5
+
+
+def test_c2c_output_guard_band():
+    """Strided output: bytes between outputs and past the span stay untouched."""
+    import plfft
+    import torch
+
+    n, hm, os_, od = 256, 3, 2, 600
+    plan = plfft.make_plan("c2c", n, hm, 1, n, os_, od)
+    x = torch.randn(hm * n, dtype=torch.complex64, device="cuda")
+    sentinel = complex(1234.5, -987.25)
+    total = (hm - 1) * od + (n - 1) * os_ + 1 + 64
+    y = torch.full((total,), sentinel, dtype=torch.complex64, device="cuda")
+    plan.execute(x.data_ptr(), y.data_ptr())
+    yc = y.cpu().numpy()
+    mask = np.ones(total, bool)
+    idx = (np.arange(hm)[:, None] * od + np.arange(n)[None, :] * os_).ravel()
+    mask[idx] = False
+    assert np.all(yc[mask] == np.complex64(sentinel))
