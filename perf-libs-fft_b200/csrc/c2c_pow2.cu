@@ -1,0 +1,499 @@
+// Power-of-two C2C FP32 kernel with a compile-time stage list.
+//
+// N = R0 * E^(S-1): stage 0 is radix R0 (no twiddles), stages 1.. are radix E.
+// T = N/E threads per transform, G transforms per CTA.  Unit-stride batches
+// are moved by the TMA engine: one bulk copy per transform into shared memory
+// (mbarrier completion, bounded wait), and one bulk copy back out after the
+// result is written over the same shared-memory slots.  Between stages the
+// data is exchanged through a padded shared-memory buffer; because every
+// index is a compile-time power of two the address arithmetic folds to
+// shifts and masks, and only the codelets this N uses are instantiated.
+//
+// This is the fast path for the reference's power-of-two C2C plans
+// (src/planner/strategies/cooley_tukey.hpp:622-679 recursion of radix-r
+// twiddle levels; here all levels of one transform stay on chip).
+#include "kernels.h"
+#include "ptx.cuh"
+#include "stockham.cuh"
+
+#include <algorithm>
+
+namespace plfft_b200 {
+
+template <int N, int E>
+struct P2 {
+  static constexpr int count_e(int m) { return (m % E == 0 && m > 1) ? 1 + count_e(m / E) : 0; }
+  static constexpr int pow_e(int k) { return k == 0 ? 1 : E * pow_e(k - 1); }
+  static constexpr int KE = count_e(N);           // number of full radix-E stages
+  static constexpr int REST = N / pow_e(KE);      // leftover factor (1 or < E)
+  static constexpr int S = KE + (REST > 1 ? 1 : 0);
+  static constexpr int R0 = REST > 1 ? REST : E;
+  static constexpr int T = N / E;
+  static constexpr int radix(int s) { return s == 0 ? R0 : E; }
+  static constexpr int ns(int s) { return s == 0 ? 1 : R0 * pow_e(s - 1); }
+  static constexpr int twoff(int s) { return s <= 1 ? 0 : twoff(s - 1) + (E - 1) * ns(s - 1); }
+};
+
+// TWS: the twiddle table lives in shared memory (plain loads) instead of
+// global memory (read-only cache loads)
+template <int T, int E, int R, int NS, int TWOFF, int DIR, bool TWS = false>
+__device__ __forceinline__ void st_bfly(float2 (&v)[E], int t, const float2* __restrict__ tw) {
+  constexpr int M = E / R;
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    float2 x[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) x[i] = v[m + M * i];
+    if constexpr (NS > 1) {
+      const int j = t + T * m;
+      const int r = j & (NS - 1);
+      const float2* w = tw + TWOFF + r;
+#pragma unroll
+      for (int i = 1; i < R; ++i) {
+        float2 wi;
+        if constexpr (TWS)
+          wi = w[(i - 1) * NS];
+        else
+          wi = __ldg(w + (i - 1) * NS);
+        x[i] = twmul<DIR>(x[i], wi);
+      }
+    }
+    dft<R, DIR>(x);
+#pragma unroll
+    for (int i = 0; i < R; ++i) v[m + M * i] = x[i];
+  }
+}
+
+template <int T, int E, int R, int NS>
+__device__ __forceinline__ void st_scatter(const float2 (&v)[E], int t, float2* sm) {
+  constexpr int M = E / R;
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const int j = t + T * m;
+    const int base = (j & ~(NS - 1)) * R + (j & (NS - 1));
+#pragma unroll
+    for (int i = 0; i < R; ++i) sm[spad(base + i * NS)] = v[m + M * i];
+  }
+}
+
+template <int N, int E, int DIR, int S, bool TWS = false>
+struct Stages {
+  using P = P2<N, E>;
+  template <class Sync>
+  __device__ __forceinline__ static void run(float2 (&v)[E], int t, float2* xb, const float2* tw, Sync sync) {
+    if constexpr (S < P::S) {
+      sync();  // the buffer's previous contents are fully read
+      st_scatter<P::T, E, P::radix(S - 1), P::ns(S - 1)>(v, t, xb);
+      sync();
+#pragma unroll
+      for (int q = 0; q < E; ++q) v[q] = xb[spad(t + P::T * q)];
+      st_bfly<P::T, E, P::radix(S), P::ns(S), P::twoff(S), DIR, TWS>(v, t, tw);
+      Stages<N, E, DIR, S + 1, TWS>::run(v, t, xb, tw, sync);
+    }
+  }
+};
+
+template <int E>
+constexpr int pow2_max_threads() { return E <= 16 ? 512 : 256; }
+
+template <int N, int E, int DIR>
+__global__ void __launch_bounds__(pow2_max_threads<E>()) c2c_pow2_kernel(const Pow2Launch L) {
+  using P = P2<N, E>;
+  constexpr int T = P::T;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ uint64_t bar;
+  const int G = L.g;
+  // one buffer per transform: bulk-copied input (natural order), then the
+  // padded stage exchanges, then the natural-order result for the bulk store
+  constexpr int PITCH = (spad_len_c(N) + 1) & ~1;  // even -> 16-byte aligned slots
+  float2* inbuf = reinterpret_cast<float2*>(smraw);
+  const int grp = threadIdx.x / T;
+  const int t = threadIdx.x - grp * T;
+  const int64_t b0 = int64_t(blockIdx.x) * G;
+  const int64_t remain = L.howmany - b0;
+  const int cnt = remain < G ? int(remain) : G;
+  const bool live = grp < cnt;
+  float2* mine = inbuf + grp * PITCH;
+  float2* xb = mine;
+
+  auto sync = [&]() {
+    if constexpr (T <= 32)
+      __syncwarp();
+    else
+      __syncthreads();
+  };
+
+  float2 v[E];
+  if (L.tma_in) {
+    if (threadIdx.x == 0) {
+      mbar_init(&bar, 1);
+      mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      mbar_arrive_expect_tx(&bar, uint32_t(cnt) * N * 8u);
+      for (int c = 0; c < cnt; ++c) bulk_g2s(inbuf + c * PITCH, L.in + (b0 + c) * L.idist, N * 8u, &bar);
+    }
+    const bool ok = mbar_wait_bounded(&bar, 0);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicExch(L.err, 1);
+      return;
+    }
+    if (live) {
+#pragma unroll
+      for (int q = 0; q < E; ++q) v[q] = mine[t + T * q];
+    } else {
+#pragma unroll
+      for (int q = 0; q < E; ++q) v[q] = make_float2(0.f, 0.f);
+    }
+  } else {
+    if (live) {
+      const float2* src = L.in + (b0 + grp) * L.idist;
+#pragma unroll
+      for (int q = 0; q < E; ++q) v[q] = src[t + T * q];
+    } else {
+#pragma unroll
+      for (int q = 0; q < E; ++q) v[q] = make_float2(0.f, 0.f);
+    }
+  }
+
+  st_bfly<T, E, P::radix(0), 1, 0, DIR>(v, t, L.tw);
+  Stages<N, E, DIR, 1>::run(v, t, xb, L.tw, sync);
+
+  const float s = L.scale;
+  if (s != 1.f) {
+#pragma unroll
+    for (int q = 0; q < E; ++q) v[q] = cscale(v[q], s);
+  }
+  if (L.tma_out) {
+    sync();  // last exchange fully read before the slots are reused
+    if (live) {
+#pragma unroll
+      for (int q = 0; q < E; ++q) mine[t + T * q] = v[q];
+    }
+    fence_proxy_async();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int c = 0; c < cnt; ++c) bulk_s2g(L.out + (b0 + c) * L.odist, inbuf + c * PITCH, N * 8u);
+      bulk_commit();
+      bulk_wait_read_all();
+    }
+  } else if (live) {
+    float2* dst = L.out + (b0 + grp) * L.odist;
+#pragma unroll
+    for (int q = 0; q < E; ++q) dst[t + T * q] = v[q];
+  }
+}
+
+// Persistent variant: each CTA owns a ring of kRing buffer slots and walks
+// the groups blockIdx.x, blockIdx.x + gridDim.x, ...  The bulk loads of the
+// next two groups are in flight while the current one is transformed, and
+// each result leaves through an asynchronous bulk store.
+constexpr int kRing = 3;
+
+template <int N, int E, int DIR>
+__global__ void __launch_bounds__(pow2_max_threads<E>()) c2c_pow2_ring_kernel(const Pow2Launch L) {
+  using P = P2<N, E>;
+  constexpr int T = P::T;
+  constexpr int PITCH = (spad_len_c(N) + 1) & ~1;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ uint64_t bar[kRing];
+  const int G = L.g;
+  const int64_t ngroups = (L.howmany + G - 1) / G;
+  const int grp = threadIdx.x / T;
+  const int t = threadIdx.x - grp * T;
+  float2* const ring = reinterpret_cast<float2*>(smraw);
+
+  auto group_of = [&](int k) { return int64_t(blockIdx.x) + int64_t(k) * gridDim.x; };
+  auto count_of = [&](int64_t g) {
+    const int64_t r = L.howmany - g * G;
+    return r < G ? int(r) : G;
+  };
+  auto slot = [&](int k) { return ring + (k % kRing) * G * PITCH; };
+  auto issue = [&](int k) {  // thread 0 only
+    const int64_t g = group_of(k);
+    if (g >= ngroups) return;
+    const int cnt = count_of(g);
+    uint64_t* b = &bar[k % kRing];
+    mbar_arrive_expect_tx(b, uint32_t(cnt) * N * 8u);
+    float2* dst = slot(k);
+    for (int c = 0; c < cnt; ++c) bulk_g2s(dst + c * PITCH, L.in + (g * G + c) * L.idist, N * 8u, b);
+  };
+  auto sync = [&]() {
+    if constexpr (T <= 32)
+      __syncwarp();
+    else
+      __syncthreads();
+  };
+
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < kRing; ++b) mbar_init(&bar[b], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    issue(0);
+    issue(1);
+  }
+  for (int k = 0; group_of(k) < ngroups; ++k) {
+    const int64_t g = group_of(k);
+    const int cnt = count_of(g);
+    const bool live = grp < cnt;
+    float2* mine = slot(k) + grp * PITCH;
+    const bool ok = mbar_wait_bounded(&bar[k % kRing], uint32_t(k / kRing) & 1u);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicExch(L.err, 1);
+      break;
+    }
+    float2 v[E];
+    if (live) {
+#pragma unroll
+      for (int q = 0; q < E; ++q) v[q] = mine[t + T * q];
+    } else {
+#pragma unroll
+      for (int q = 0; q < E; ++q) v[q] = make_float2(0.f, 0.f);
+    }
+    st_bfly<T, E, P::radix(0), 1, 0, DIR>(v, t, L.tw);
+    Stages<N, E, DIR, 1>::run(v, t, mine, L.tw, sync);
+    const float s = L.scale;
+    if (s != 1.f) {
+#pragma unroll
+      for (int q = 0; q < E; ++q) v[q] = cscale(v[q], s);
+    }
+    sync();
+    if (live) {
+#pragma unroll
+      for (int q = 0; q < E; ++q) mine[t + T * q] = v[q];
+    }
+    fence_proxy_async();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const float2* src = slot(k);
+      for (int c = 0; c < cnt; ++c) bulk_s2g(L.out + (g * G + c) * L.odist, src + c * PITCH, N * 8u);
+      bulk_commit();
+      bulk_wait_read_but1();  // the slot of group k-1 is free again
+      issue(k + 2);
+    }
+  }
+  if (threadIdx.x == 0) bulk_wait_read_all();
+}
+
+// Warp-group variant: a persistent CTA holds GP independent groups of
+// W = T/32 warps; each group transforms one sequence at a time through its
+// own ring of NS shared-memory slots, with its own mbarriers and producer
+// lane, so groups never wait on each other.  Group-local synchronisation is
+// __syncwarp (W == 1) or a named barrier.  The stage twiddles are copied to
+// shared memory once per CTA.  The refill of a slot is issued one iteration
+// after its bulk store, so the store has drained before the slot is reused.
+constexpr int kMaxGroups = 15;
+
+template <int N, int E, int DIR, int NS>
+__global__ void __launch_bounds__(512, 1) c2c_pow2_group_kernel(const Pow2Launch L) {
+  using P = P2<N, E>;
+  constexpr int T = P::T;
+  static_assert(T % 32 == 0, "group kernel needs whole warps");
+  constexpr int W = T / 32;
+  constexpr int PITCH = (spad_len_c(N) + 1) & ~1;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ uint64_t bar[kMaxGroups][NS];
+  __shared__ int64_t meta[kMaxGroups][NS];  // transform held by each slot
+  __shared__ int next;                      // CTA-local work counter
+  const int grp = threadIdx.x / T;
+  const int t = threadIdx.x - grp * T;
+  float2* tws = reinterpret_cast<float2*>(smraw);
+  float2* slots = tws + L.tw_len + ((L.tw_len & 1) ? 1 : 0);
+  float2* myslots = slots + grp * NS * PITCH;
+  // this CTA's contiguous share of the batch
+  const int64_t lo = L.howmany * blockIdx.x / gridDim.x;
+  const int64_t hi = L.howmany * (blockIdx.x + 1) / gridDim.x;
+  const bool producer = (t == 0);
+
+  auto gsync = [&]() {
+    if constexpr (W == 1)
+      __syncwarp();
+    else
+      asm volatile("bar.sync %0, %1;" ::"r"(grp + 1), "r"(T) : "memory");
+  };
+  // producer: claim the next transform of this CTA and start its load into
+  // slot s (or mark the slot as the end of the group's work)
+  auto fetch = [&](int s) {
+    const int64_t b = lo + atomicAdd(&next, 1);
+    meta[grp][s] = b;
+    uint64_t* br = &bar[grp][s];
+    if (b < hi) {
+      mbar_arrive_expect_tx(br, N * 8u);
+      bulk_g2s(myslots + s * PITCH, L.in + b * L.idist, N * 8u, br);
+    } else {
+      mbar_arrive(br);
+    }
+  };
+
+  if (threadIdx.x == 0) next = 0;
+  if (producer) {
+    for (int s = 0; s < NS; ++s) mbar_init(&bar[grp][s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  // start the rings first, then stage the twiddles while the loads fly
+  if (producer)
+    for (int s = 0; s < NS; ++s) fetch(s);
+  for (int i = threadIdx.x; i < L.tw_len; i += blockDim.x) tws[i] = L.tw[i];
+  __syncthreads();
+
+  for (int k = 0;; ++k) {
+    const int s = k % NS;
+    const bool ok = mbar_wait_bounded(&bar[grp][s], uint32_t(k / NS) & 1u);
+    bool failed;
+    if constexpr (W == 1) {
+      failed = __any_sync(0xffffffffu, !ok);
+    } else {
+      uint32_t any;
+      asm volatile(
+          "{\n\t.reg .pred p, q;\n\t"
+          "setp.ne.u32 p, %1, 0;\n\t"
+          "bar.red.or.pred q, %2, %3, p;\n\t"
+          "selp.u32 %0, 1, 0, q;\n\t}"
+          : "=r"(any)
+          : "r"(ok ? 0u : 1u), "r"(grp + 1), "r"(T)
+          : "memory");
+      failed = any != 0;
+    }
+    if (failed) {
+      if (producer) atomicExch(L.err, 1);
+      break;  // group-local exit; other groups are independent
+    }
+    const int64_t b = meta[grp][s];
+    if (b >= hi) break;
+    float2* mine = myslots + s * PITCH;
+    float2 v[E];
+#pragma unroll
+    for (int q = 0; q < E; ++q) v[q] = mine[t + T * q];
+    st_bfly<T, E, P::radix(0), 1, 0, DIR, true>(v, t, tws);
+    // the slot used by iteration k-1 has had a full stage to drain its store
+    if (k >= 1 && producer) {
+      bulk_wait_read_all();
+      fetch((k - 1) % NS);
+    }
+    Stages<N, E, DIR, 1, true>::run(v, t, mine, tws, gsync);
+    const float sc = L.scale;
+    if (sc != 1.f) {
+#pragma unroll
+      for (int q = 0; q < E; ++q) v[q] = cscale(v[q], sc);
+    }
+    gsync();
+#pragma unroll
+    for (int q = 0; q < E; ++q) mine[t + T * q] = v[q];
+    fence_proxy_async();
+    gsync();
+    if (producer) {
+      bulk_s2g(L.out + b * L.odist, mine, N * 8u);
+      bulk_commit();
+    }
+  }
+  if (producer) bulk_wait_read_all();
+}
+
+int pow2_smem_bytes(int n, int g) { return g * ((spad_len(n) + 1) & ~1) * int(sizeof(float2)); }
+
+static int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 1;
+  }
+  return n;
+}
+
+template <int N, int E, int DIR>
+static cudaError_t run_pow2(const Pow2Launch& L, cudaStream_t st) {
+  const int threads = (N / E) * L.g;
+  const int64_t ngroups = (L.howmany + L.g - 1) / L.g;
+  if constexpr ((N / E) % 32 == 0) {
+    if (L.tma_in && L.tma_out && L.ring >= 2) {
+      constexpr int T = N / E;
+      constexpr int PITCH = (spad_len_c(N) + 1) & ~1;
+      const int ns = L.ring == 3 ? 3 : 2;
+      const int per_group = ns * PITCH * 8;
+      const int tw_bytes = ((L.tw_len + 1) & ~1) * 8;
+      int gp = (227 * 1024 - 1024 - tw_bytes) / per_group;
+      gp = std::min(gp, std::min(kMaxGroups, 512 / T));
+      if (L.gp > 0) gp = std::min(gp, L.gp);  // explicit cap from the planner
+      if (gp >= 1) {
+        const int smem = tw_bytes + gp * per_group;
+        const int64_t want_groups = L.howmany;
+        const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(sm_count(), (want_groups + gp - 1) / gp));
+        auto launch = [&](auto kern) {
+          cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+          if (e != cudaSuccess) return e;
+          kern<<<dim3(unsigned(grid)), dim3(gp * T), smem, st>>>(L);
+          return cudaGetLastError();
+        };
+        return ns == 3 ? launch(c2c_pow2_group_kernel<N, E, DIR, 3>) : launch(c2c_pow2_group_kernel<N, E, DIR, 2>);
+      }
+    }
+  }
+  if (L.tma_in && L.tma_out && L.ring) {
+    auto* k = c2c_pow2_ring_kernel<N, E, DIR>;
+    const int smem = kRing * pow2_smem_bytes(N, L.g);
+    if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      if (e != cudaSuccess) return e;
+    }
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    // k groups per CTA so that the grid is one resident wave
+    const int64_t cap = int64_t(per_sm) * sm_count();
+    const int64_t per_cta = (ngroups + cap - 1) / cap;
+    const int64_t grid = (ngroups + per_cta - 1) / per_cta;
+    k<<<dim3(unsigned(grid)), dim3(threads), smem, st>>>(L);
+    return cudaGetLastError();
+  }
+  const int smem = pow2_smem_bytes(N, L.g);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(c2c_pow2_kernel<N, E, DIR>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+  }
+  c2c_pow2_kernel<N, E, DIR><<<dim3(unsigned(ngroups)), dim3(threads), smem, st>>>(L);
+  return cudaGetLastError();
+}
+
+template <int N, int E>
+static cudaError_t run_pow2_dir(int dir, const Pow2Launch& L, cudaStream_t st) {
+  return dir < 0 ? run_pow2<N, E, -1>(L, st) : run_pow2<N, E, 1>(L, st);
+}
+
+bool pow2_supported(int n, int e) {
+  if (e != 16 && e != 32) return false;
+  if (n < 64 || n > 8192 || (n & (n - 1))) return false;
+  return n / e <= (e <= 16 ? 512 : 256);
+}
+
+cudaError_t launch_c2c_pow2(int n, int e, int dir, const Pow2Launch& L, cudaStream_t st) {
+#define PLFFT_B200_P2(NV, EV) \
+  if (n == NV && e == EV) return run_pow2_dir<NV, EV>(dir, L, st);
+  PLFFT_B200_P2(64, 16)
+  PLFFT_B200_P2(128, 16)
+  PLFFT_B200_P2(256, 16)
+  PLFFT_B200_P2(512, 16)
+  PLFFT_B200_P2(1024, 16)
+  PLFFT_B200_P2(2048, 16)
+  PLFFT_B200_P2(4096, 16)
+  PLFFT_B200_P2(8192, 16)
+  PLFFT_B200_P2(64, 32)
+  PLFFT_B200_P2(128, 32)
+  PLFFT_B200_P2(256, 32)
+  PLFFT_B200_P2(512, 32)
+  PLFFT_B200_P2(1024, 32)
+  PLFFT_B200_P2(2048, 32)
+  PLFFT_B200_P2(4096, 32)
+  PLFFT_B200_P2(8192, 32)
+#undef PLFFT_B200_P2
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace plfft_b200

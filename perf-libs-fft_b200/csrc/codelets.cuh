@@ -27,16 +27,26 @@ struct cf {
   float x, y;
 };
 
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Complex arithmetic on float2.  sm_100 executes two FP32 lanes per
+// instruction (FADD2/FMUL2/FFMA2), so re and im share one instruction.
+// a - b is formed as fma(b, -1, a): exact negation, one rounding, the same
+// result as a subtraction.
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+  return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+}
+// a * b = (a.x b.x - a.y b.y, a.x b.y + a.y b.x)
+//       = a.x * (b.x, b.y) + a.y * (-b.y, b.x)
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+  const float2 t = __fmul2_rn(make_float2(a.x, a.x), b);
+  return __ffma2_rn(make_float2(a.y, a.y), make_float2(-b.y, b.x), t);
 }
-// a * conj(b)
+// a * conj(b) = a.x * (b.x, -b.y) + a.y * (b.y, b.x)
 __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
-  return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
+  const float2 t = __fmul2_rn(make_float2(a.x, a.x), make_float2(b.x, -b.y));
+  return __ffma2_rn(make_float2(a.y, a.y), make_float2(b.y, b.x), t);
 }
-__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
 // multiply by (s * i) where s = +1 or -1 (compile time)
 template <int S>
 __device__ __forceinline__ float2 cmul_i(float2 a) {
@@ -161,10 +171,8 @@ __device__ __forceinline__ void dft_odd(float2* v) {
       constexpr int k = decltype(kc)::value;
       constexpr float c = RootCos<R, (m * k) % R>::v;
       constexpr float s = RootSin<R, (m * k) % R>::v;
-      A.x = fmaf(a[k].x, c, A.x);
-      A.y = fmaf(a[k].y, c, A.y);
-      B.x = fmaf(b[k].x, s, B.x);
-      B.y = fmaf(b[k].y, s, B.y);
+      A = __ffma2_rn(a[k], make_float2(c, c), A);
+      B = __ffma2_rn(b[k], make_float2(s, s), B);
     });
     // s*i*B with s = DIR
     float2 iB = cmul_i<DIR>(B);

@@ -54,10 +54,86 @@ struct TileLaunch {
                   // col = g % ia.ncols), if post.n != 0
 };
 
+// Static power-of-two C2C launch (c2c_pow2.cu): unit element stride,
+// transforms idist/odist apart, G per CTA; bulk copies when aligned.
+struct Pow2Launch {
+  const float2* in;
+  float2* out;
+  int64_t howmany;
+  int64_t idist, odist;
+  int g;
+  float scale;
+  const float2* tw;
+  int tw_len;  // entries in tw
+  int tma_in, tma_out;
+  int ring;  // 0 one-shot CTAs, 1 CTA ring, 2/3 warp-group rings (slots)
+  int gp;    // warp-group kernel: groups per CTA (0 = as many as fit)  // persistent ring-buffered variant
+  int* err;  // set to 1 if a bounded device wait ran out
+};
+
+// Real-data transforms through a complex DFT of length `len`
+// (realwrap.cu): pre-kernel builds the complex sequence in `work`, a C2C plan
+// transforms it in place, the post-kernel extracts the outputs.
+enum RealWrapKind {
+  RW_R2C = 0,
+  RW_C2R = 1,
+  RW_DCT1 = 2,
+  RW_DCT2 = 3,
+  RW_DCT3 = 4,
+  RW_DCT4 = 5,
+  RW_DST1 = 6,
+  RW_DST2 = 7,
+  RW_DST3 = 8,
+  RW_DST4 = 9,
+  RW_DHT = 10,
+  RW_R2HC = 11,
+  RW_HC2R = 12
+};
+struct RealWrapLaunch {
+  const void* in;
+  void* out;
+  float2* work;  // [chunk][len] complex
+  int64_t n, len, nout;
+  int64_t istride, idist, ostride, odist;
+  float scale;
+};
+cudaError_t launch_realwrap(bool pre, int kind, const RealWrapLaunch& L, int64_t m0, int64_t cnt,
+                            cudaStream_t st);
+
+// Rader / Bluestein elementwise passes (conv.cu).  n: transform length,
+// m: convolution length (M for Bluestein, P-1 for Rader).
+enum ConvStep {
+  CONV_BS_PRE = 0,
+  CONV_MUL = 1,
+  CONV_MUL_SAVE0 = 2,
+  CONV_BS_POST = 3,
+  CONV_RD_PRE = 4,
+  CONV_RD_POST = 5
+};
+struct ConvLaunch {
+  const float2* in;
+  float2* out;
+  float2* work;   // [chunk][m]
+  float2* sum0;   // [chunk] (Rader: A[0] per member)
+  const float2* chirp;  // Bluestein w_k, k < n
+  const float2* spec;   // convolution spectrum, m entries
+  const int* perm_in;   // Rader g^q mod P
+  const int* perm_out;  // Rader g^-q mod P
+  int64_t n, m;
+  int64_t istride, idist, ostride, odist;
+  float scale;
+};
+cudaError_t launch_conv(int step, const ConvLaunch& L, int64_t m0, int64_t cnt, cudaStream_t st);
+
 // kernel entry points (c2c.cu)
 cudaError_t launch_c2c_reg(int e, int dir, const RegLaunch& L, cudaStream_t st);
 cudaError_t launch_c2c_tile(int maxe, int dir, const TileLaunch& L, cudaStream_t st);
 int reg_smem_bytes(int n, int g);
 int tile_smem_bytes(int ld, int c);
+
+// c2c_pow2.cu
+bool pow2_supported(int n, int e);
+int pow2_smem_bytes(int n, int g);
+cudaError_t launch_c2c_pow2(int n, int e, int dir, const Pow2Launch& L, cudaStream_t st);
 
 }  // namespace plfft_b200

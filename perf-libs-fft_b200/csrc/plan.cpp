@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <sstream>
 
 namespace plfft_b200 {
@@ -122,9 +123,15 @@ struct RegChoice {
   std::vector<int> radices;
 };
 
+static int env_int(const char* name, int dflt) {
+  const char* v = std::getenv(name);
+  return v ? std::atoi(v) : dflt;
+}
+
 static bool choose_reg(int64_t n, RegChoice& rc) {
   if (!is_pow2(n) || n < 64 || n > kMaxOnChip) return false;
-  rc.e = n >= 1024 ? 32 : 16;
+  rc.e = env_int("PLFFT_B200_REG_E", n >= 1024 ? 32 : 16);
+  if (n / rc.e > 256) return false;  // CTA limit of the register kernel
   int64_t rest = n;
   std::vector<int> big;
   while (rest % rc.e == 0 && rest >= rc.e) {
@@ -135,7 +142,8 @@ static bool choose_reg(int64_t n, RegChoice& rc) {
   if (rest > 1) rc.radices.push_back(int(rest));
   rc.radices.insert(rc.radices.end(), big.begin(), big.end());
   rc.t = int(n / rc.e);
-  rc.g = std::max(1, 256 / rc.t);
+  rc.g = env_int("PLFFT_B200_REG_G", std::max(1, 256 / rc.t));
+  if (rc.g * rc.t > 256) rc.g = std::max(1, 256 / rc.t);
   while (rc.g > 1 && reg_smem_bytes(int(n), rc.g) > 100 * 1024) rc.g /= 2;
   return true;
 }
@@ -160,6 +168,79 @@ struct C2CRegNode : Node {
     return o.str();
   }
 };
+
+// ---------------------------------------------------------------------------
+// static power-of-two C2C node (bulk-copy staged, compile-time radices)
+// ---------------------------------------------------------------------------
+struct C2CPow2Node : Node {
+  Pow2Launch base{};
+  int n = 0, e = 0, dir = -1;
+  DevBuf tw, err;
+  cudaError_t run(const void* in, void* out, void*, cudaStream_t st) const override {
+    Pow2Launch L = base;
+    L.in = static_cast<const float2*>(in);
+    L.out = static_cast<float2*>(out);
+    const bool dist_in_ok = L.howmany == 1 || (L.idist % 2) == 0;
+    const bool dist_out_ok = L.howmany == 1 || (L.odist % 2) == 0;
+    L.tma_in = (reinterpret_cast<uintptr_t>(in) % 16 == 0) && dist_in_ok;
+    L.tma_out = (reinterpret_cast<uintptr_t>(out) % 16 == 0) && dist_out_ok;
+    return launch_c2c_pow2(n, e, dir, L, st);
+  }
+  std::string describe() const override {
+    std::ostringstream o;
+    o << "(c2c-pow2 n=" << n << " e=" << e << " g=" << base.g << (base.ring ? " ring" : "") << " bulk-copy)";
+    return o.str();
+  }
+};
+
+static int pow2_default_e(int64_t n) {
+  if (n <= 512) return 16;
+  if (n <= 2048) return 32;
+  if (n == 4096) return 16;
+  return 32;
+}
+
+static std::unique_ptr<Node> make_pow2(int64_t n, const Layout& lay, int dir, float scale, std::string* why) {
+  int e = env_int("PLFFT_B200_POW2_E", pow2_default_e(n));
+  if (!pow2_supported(int(n), e)) e = pow2_default_e(n);
+  if (!pow2_supported(int(n), e)) return nullptr;
+  auto node = std::make_unique<C2CPow2Node>();
+  node->n = int(n);
+  node->e = e;
+  node->dir = dir;
+  // radices: leftover factor first, then radix-e stages
+  std::vector<int> radices;
+  int64_t rest = n;
+  int ke = 0;
+  while (rest % e == 0 && rest > 1) {
+    rest /= e;
+    ++ke;
+  }
+  if (rest > 1) radices.push_back(int(rest));
+  for (int i = 0; i < ke; ++i) radices.push_back(e);
+  std::vector<float2> tw;
+  make_desc(int(n), radices, tw);
+  if (node->tw.upload(tw) != cudaSuccess || node->err.alloc(sizeof(int)) != cudaSuccess ||
+      cudaMemset(node->err.p, 0, sizeof(int)) != cudaSuccess) {
+    if (why) *why = "device allocation failed";
+    return nullptr;
+  }
+  const int t = int(n / e);
+  int g = std::max(1, env_int("PLFFT_B200_POW2_G", std::max(1, 128 / t)));
+  const int maxthr = e <= 16 ? 512 : 256;
+  while (g > 1 && (g * t > maxthr || pow2_smem_bytes(int(n), g) > 200 * 1024)) g /= 2;
+  node->base.howmany = lay.howmany;
+  node->base.idist = lay.idist;
+  node->base.odist = lay.odist;
+  node->base.g = g;
+  node->base.scale = scale;
+  node->base.tw = node->tw.as<float2>();
+  node->base.tw_len = int(tw.size());
+  node->base.err = node->err.as<int>();
+  node->base.ring = env_int("PLFFT_B200_POW2_RING", 3);
+  node->base.gp = std::max(0, env_int("PLFFT_B200_POW2_GP", 0));
+  return node;
+}
 
 // ---------------------------------------------------------------------------
 // shared-memory tile C2C node (any smooth n <= kMaxOnChip, any strides)
@@ -346,6 +427,10 @@ std::unique_ptr<Node> make_c2c_node(int64_t n, const Layout& lay, int dir, float
   const bool unit = lay.istride == 1 && lay.ostride == 1;
   const bool interleaved = !unit && (lay.howmany > 1) &&
                            (std::llabs(lay.idist) < lay.istride || std::llabs(lay.odist) < lay.ostride);
+  if (unit && !std::getenv("PLFFT_B200_NO_POW2")) {
+    auto p2 = make_pow2(n, lay, dir, scale, why);
+    if (p2) return p2;
+  }
   RegChoice rc;
   if (unit && choose_reg(n, rc)) {
     auto node = std::make_unique<C2CRegNode>();
@@ -372,11 +457,11 @@ std::unique_ptr<Node> make_c2c_node(int64_t n, const Layout& lay, int dir, float
   if (n <= kMaxOnChip && is_smooth(n)) {
     Addr ia{lay.idist, 0, lay.istride, 1};
     Addr oa{lay.odist, 0, lay.ostride, 1};
-    return make_tile(n, lay.howmany, ia, oa, dir, scale, interleaved, why);
+    auto t = make_tile(n, lay.howmany, ia, oa, dir, scale, interleaved, why);
+    if (t) return t;
   }
   if (is_smooth(n)) return make_four_step(n, lay, dir, scale, why);
-  if (why) *why = "length " + std::to_string(n) + " needs a convolution schedule";
-  return nullptr;
+  return make_conv_node(n, lay, dir, scale, why);
 }
 
 PlanData::~PlanData() {

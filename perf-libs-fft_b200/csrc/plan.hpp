@@ -108,6 +108,14 @@ constexpr int kMaxOnChip = 16384;
 std::unique_ptr<Node> make_c2c_node(int64_t n, const Layout& lay, int dir, float scale,
                                     int precision, std::string* why);
 
+// Rader (prime n, smooth n-1) or Bluestein (any n) convolution node.
+std::unique_ptr<Node> make_conv_node(int64_t n, const Layout& lay, int dir, float scale, std::string* why);
+int64_t next_smooth(int64_t n);
+
+// R2C / C2R / R2R through a C2C plan of a related length (realwrap.cu);
+// kind is a RealWrapKind.
+std::unique_ptr<Node> make_realwrap_node(int kind, int64_t n, const Layout& lay, float scale, std::string* why);
+
 // The plan object behind plfft_plan_t.
 struct PlanData {
   ConfigData cfg;

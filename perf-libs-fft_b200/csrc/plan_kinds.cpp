@@ -46,10 +46,24 @@ plfft_status_t build_plan(PlanData& p, std::string* why) {
       case TKind::C2C:
         p.root = make_c2c_node(c.n, lay, c.payload, scale, c.precision, why);
         break;
-      default:
-        if (why) *why = "transform kind not built yet";
+      case TKind::R2C:
+        p.root = make_realwrap_node(RW_R2C, c.n, lay, scale, why);
         break;
+      case TKind::C2R:
+        p.root = make_realwrap_node(RW_C2R, c.n, lay, scale, why);
+        break;
+      case TKind::R2R: {
+        // plfft_r2r_kind_t -> RealWrapKind
+        static const int map[] = {RW_DCT1, RW_DCT2, RW_DCT3, RW_DCT4, RW_DST1, RW_DST2,
+                                  RW_DST3, RW_DST4, RW_DHT,  RW_R2HC, RW_HC2R};
+        p.root = make_realwrap_node(map[c.payload], c.n, lay, scale, why);
+        break;
+      }
     }
+  } else if ((c.data_type == PLFFT_DATA_TYPE_Q15 || c.data_type == PLFFT_DATA_TYPE_Q7) &&
+             c.kind == TKind::R2R) {
+    // fixed-point real-to-real has no implementation (reference src/plfft.cpp:248-261)
+    if (why) *why = "fixed-point R2R is not supported";
   } else {
     if (why) *why = "data type not supported on the device path";
   }

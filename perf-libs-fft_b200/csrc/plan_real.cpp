@@ -1,0 +1,104 @@
+// Plan nodes for R2C, C2R and R2R built on a C2C plan (realwrap.cu).
+#include <algorithm>
+#include <sstream>
+
+#include "plan.hpp"
+
+namespace plfft_b200 {
+
+namespace {
+
+struct RealWrapNode : Node {
+  int kind = 0;
+  int64_t n = 0, len = 0, nout = 0;
+  Layout lay{};
+  float scale = 1.f;
+  int64_t chunk = 1;
+  std::unique_ptr<Node> inner;  // C2C of length len over `chunk` contiguous members, in place
+  size_t inner_ws() const { return inner->workspace(); }
+  size_t workspace() const override {
+    const size_t work = size_t(chunk) * size_t(len) * sizeof(float2);
+    return ((work + 255) & ~size_t(255)) + inner_ws();
+  }
+  int launches() const override {
+    const int64_t chunks = (lay.howmany + chunk - 1) / chunk;
+    return int(chunks * (2 + inner->launches()));
+  }
+  cudaError_t run(const void* in, void* out, void* ws, cudaStream_t st) const override {
+    float2* work = static_cast<float2*>(ws);
+    const size_t work_bytes = (size_t(chunk) * size_t(len) * sizeof(float2) + 255) & ~size_t(255);
+    void* iws = static_cast<char*>(ws) + work_bytes;
+    RealWrapLaunch L{in, out, work, n, len, nout, lay.istride, lay.idist, lay.ostride, lay.odist, scale};
+    for (int64_t m0 = 0; m0 < lay.howmany; m0 += chunk) {
+      const int64_t cnt = std::min(chunk, lay.howmany - m0);
+      cudaError_t e = launch_realwrap(true, kind, L, m0, cnt, st);
+      if (e != cudaSuccess) return e;
+      e = run_inner(cnt, work, iws, st);
+      if (e != cudaSuccess) return e;
+      e = launch_realwrap(false, kind, L, m0, cnt, st);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+  // the inner plan was built for `chunk` members; the last chunk may be
+  // shorter, which only changes which members hold meaningful data
+  cudaError_t run_inner(int64_t, float2* work, void* iws, cudaStream_t st) const {
+    return inner->run(work, work, iws, st);
+  }
+  std::string describe() const override {
+    static const char* names[] = {"r2c", "c2r", "dct1", "dct2", "dct3", "dct4", "dst1",
+                                  "dst2", "dst3", "dst4", "dht", "r2hc", "hc2r"};
+    std::ostringstream o;
+    o << "(" << names[kind] << "-via-c2c n=" << n << " len=" << len << " chunk=" << chunk << " "
+      << inner->describe() << ")";
+    return o.str();
+  }
+};
+
+int64_t wrap_len(int kind, int64_t n) {
+  switch (kind) {
+    case RW_DCT1: return 2 * (n - 1);
+    case RW_DST1: return 2 * (n + 1);
+    case RW_DCT2:
+    case RW_DCT3:
+    case RW_DCT4:
+    case RW_DST2:
+    case RW_DST3:
+    case RW_DST4: return 2 * n;
+    default: return n;
+  }
+}
+
+int wrap_dir(int kind) {
+  switch (kind) {
+    case RW_C2R:
+    case RW_HC2R:
+    case RW_DCT3:
+    case RW_DST3: return +1;
+    default: return -1;
+  }
+}
+
+}  // namespace
+
+std::unique_ptr<Node> make_realwrap_node(int kind, int64_t n, const Layout& lay, float scale, std::string* why) {
+  if (kind == RW_DCT1 && n < 2) {
+    if (why) *why = "DCT-I needs n > 1";
+    return nullptr;
+  }
+  auto node = std::make_unique<RealWrapNode>();
+  node->kind = kind;
+  node->n = n;
+  node->len = wrap_len(kind, n);
+  node->nout = kind == RW_R2C ? n / 2 + 1 : n;
+  node->lay = lay;
+  node->scale = scale;
+  const int64_t target = 64ll << 20;  // bytes of complex work per chunk
+  node->chunk = std::max<int64_t>(1, std::min<int64_t>(lay.howmany, target / (node->len * 8)));
+  Layout inner{node->chunk, 1, node->len, 1, node->len};
+  node->inner = make_c2c_node(node->len, inner, wrap_dir(kind), 1.0f, 0, why);
+  if (!node->inner) return nullptr;
+  return node;
+}
+
+}  // namespace plfft_b200

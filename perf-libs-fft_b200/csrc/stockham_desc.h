@@ -25,4 +25,6 @@ __host__ __device__
 #endif
 int spad_len(int n) { return (n + (n >> 4)) | 1; }
 
+constexpr int spad_len_c(int n) { return (n + (n >> 4)) | 1; }
+
 }  // namespace plfft_b200

@@ -40,6 +40,28 @@ def test_c2c_reference_layouts(case, direction):
     assert oracle.rel_l2(got, ref) <= oracle.fp32_tol(n), plan.describe()
 
 
+# reference test/c2c_f32.cpp:17,24 -- prime and large-prime-factor layouts
+REF_CONV_CASES = [(23, 49, 441, 9, 441, 9), (1058, 4, 1058, 1, 1058, 1), (23, 3, 1, 23, 1, 23)]
+
+
+@pytest.mark.parametrize("case", REF_CONV_CASES)
+@pytest.mark.parametrize("direction", [-1, 1])
+def test_c2c_reference_conv_layouts(case, direction):
+    n, hm, is_, id_, os_, od = case
+    got, ref, plan = c2c_case(n, hm, is_, id_, os_, od, direction=direction, seed=17)
+    assert oracle.rel_l2(got, ref) <= oracle.fp32_tol(n), plan.describe()
+
+
+@pytest.mark.parametrize("n", [17, 23, 97, 1009, 4099, 1031, 1058, 2 * 8191, 65537, 8191 * 3])
+@pytest.mark.parametrize("direction", [-1, 1])
+def test_c2c_rader_bluestein(n, direction):
+    howmany = 3
+    got, ref, plan = c2c_case(n, howmany, direction=direction, seed=n, method="fft")
+    expect = "rader" if n in (17, 23, 97, 1009, 65537) else "bluestein"
+    assert expect in plan.describe(), plan.describe()
+    assert oracle.rel_l2(got, ref) <= oracle.fp32_tol(n), plan.describe()
+
+
 @pytest.mark.parametrize("n", [32768, 65536, 1 << 18, 1 << 20])
 def test_c2c_four_step(n):
     howmany = 2

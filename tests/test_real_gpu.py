@@ -1,0 +1,141 @@
+"""R2C / C2R / R2R FP32 parity: CUDA path (C-ABI) vs the FP64 oracle.
+
+Gate: rel-L2 <= 4*log2(N)*2^-24.  Cases follow the reference's real-data
+tests (test/simple_test.hpp:16-95 round trips and sums, test/r2r_test.hpp:
+82-178 all 11 kinds, test/plfft_interface_test.cpp:360-413 in-place R2C/C2R).
+"""
+import numpy as np
+import pytest
+
+import oracle
+import plfft
+from helpers import gather, span
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def run_plan(plan, x, nout_elems, out_dtype):
+    import torch
+
+    d = _dev(x)
+    y = torch.zeros(nout_elems, dtype=out_dtype, device="cuda")
+    plan.execute(d.data_ptr(), y.data_ptr())
+    return y.cpu().numpy()
+
+
+R2C_SIZES = [1, 2, 3, 4, 5, 8, 16, 17, 64, 100, 128, 1000, 1024, 4096, 8192, 32768]
+
+
+@pytest.mark.parametrize("n", R2C_SIZES)
+def test_r2c(n):
+    import torch
+
+    hm = max(1, min(32, 65536 // n))
+    h = n // 2 + 1
+    rng = np.random.default_rng(n)
+    x = rng.uniform(-1, 1, hm * n).astype(np.float32)
+    plan = plfft.make_plan("r2c", n, hm)
+    y = run_plan(plan, x, hm * h, torch.complex64).reshape(hm, h)
+    ref = oracle.r2c(x.reshape(hm, n).astype(np.float64))
+    assert oracle.rel_l2(y, ref) <= oracle.fp32_tol(n), plan.describe()
+
+
+@pytest.mark.parametrize("n", R2C_SIZES)
+def test_c2r(n):
+    import torch
+
+    hm = max(1, min(32, 65536 // n))
+    h = n // 2 + 1
+    rng = np.random.default_rng(n + 1)
+    X = (rng.uniform(-1, 1, (hm, h)) + 1j * rng.uniform(-1, 1, (hm, h))).astype(np.complex64)
+    plan = plfft.make_plan("c2r", n, hm)
+    y = run_plan(plan, X.ravel(), hm * n, torch.float32).reshape(hm, n)
+    ref = oracle.c2r(X.astype(np.complex128), n)
+    assert oracle.rel_l2(y, ref) <= oracle.fp32_tol(n), plan.describe()
+
+
+@pytest.mark.parametrize("n", [4096, 1000, 17])
+def test_r2c_c2r_round_trip_scaled(n):
+    import torch
+
+    hm = 8
+    h = n // 2 + 1
+    rng = np.random.default_rng(9)
+    x = rng.uniform(-1, 1, hm * n).astype(np.float32)
+    f = plfft.make_plan("r2c", n, hm)
+    b = plfft.make_plan("c2r", n, hm, scale=1.0 / n)
+    d = _dev(x)
+    y = torch.empty(hm * h, dtype=torch.complex64, device="cuda")
+    z = torch.empty(hm * n, dtype=torch.float32, device="cuda")
+    f.execute(d.data_ptr(), y.data_ptr())
+    b.execute(y.data_ptr(), z.data_ptr())
+    assert oracle.rel_l2(z.cpu().numpy(), x) <= oracle.fp32_tol(n)
+
+
+@pytest.mark.parametrize("n", [4, 5])
+def test_in_place_real_complex_round_trip(n):
+    """reference test/plfft_interface_test.cpp:360-413 (spans 6 real / 3 complex)."""
+    hm, rspan, cspan = 2, 6, 3
+    data = np.zeros(hm * rspan, np.float32)
+    for b in range(hm):
+        for e in range(n):
+            data[b * rspan + e] = b * 10 + e + 1
+    expected = data.copy() * n
+    f = plfft.make_plan("r2c", n, hm, 1, rspan, 1, cspan, alias=plfft.IoAlias.MAY_ALIAS)
+    c = plfft.make_plan("c2r", n, hm, 1, cspan, 1, rspan, alias=plfft.IoAlias.MAY_ALIAS)
+    f.execute(data.ctypes.data, data.ctypes.data)
+    c.execute(data.ctypes.data, data.ctypes.data)
+    for b in range(hm):
+        for e in range(n):
+            i = b * rspan + e
+            assert abs(data[i] - expected[i]) < 1e-4
+
+
+KINDS = ["DCT_1", "DCT_2", "DCT_3", "DCT_4", "DST_1", "DST_2", "DST_3", "DST_4", "DHT", "R2HC", "HC2R"]
+
+
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("n", [2, 3, 8, 17, 64, 128, 1024])
+def test_r2r(kind, n):
+    import torch
+
+    hm = 4
+    rng = np.random.default_rng(hash((kind, n)) % 2**32)
+    x = rng.uniform(-1, 1, hm * n).astype(np.float32)
+    plan = plfft.make_plan("r2r", n, hm, r2r_kind=plfft.R2RKind[kind])
+    y = run_plan(plan, x, hm * n, torch.float32).reshape(hm, n)
+    ref = oracle.r2r(x.reshape(hm, n).astype(np.float64), kind)
+    assert oracle.rel_l2(y, ref) <= oracle.fp32_tol(2 * n), (kind, n, plan.describe())
+
+
+def test_dct1_n1_rejected():
+    with pytest.raises(plfft.PlfftError) as e:
+        plfft.make_plan("r2r", 1, 1, r2r_kind=plfft.R2RKind.DCT_1)
+    assert e.value.status == plfft.Status.PLAN_CREATION_FAILED
+
+
+def test_r2r_in_place_r2hc():
+    """reference test/plfft_interface_test.cpp:415-433."""
+    data = np.array([1, 2, 3, 4], np.float32)
+    p = plfft.make_plan("r2r", 4, 1, r2r_kind=plfft.R2RKind.R2HC, alias=plfft.IoAlias.MAY_ALIAS)
+    p.execute(data.ctypes.data, data.ctypes.data)
+    assert data[0] == 10.0
+
+
+@pytest.mark.parametrize("kind", ["DCT_2", "DST_2"])
+def test_r2r_strided(kind):
+    import torch
+
+    n, hm, is_, id_, os_, od = 64, 3, 2, 200, 3, 300
+    rng = np.random.default_rng(5)
+    x = rng.uniform(-1, 1, span(hm, id_, n, is_)).astype(np.float32)
+    plan = plfft.make_plan("r2r", n, hm, is_, id_, os_, od, r2r_kind=plfft.R2RKind[kind])
+    y = run_plan(plan, x, span(hm, od, n, os_), torch.float32)
+    ref = oracle.r2r(gather(x, hm, id_, n, is_).astype(np.float64), kind)
+    assert oracle.rel_l2(gather(y, hm, od, n, os_), ref) <= oracle.fp32_tol(2 * n)
