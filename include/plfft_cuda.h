@@ -60,6 +60,34 @@ plfft_status_t plfft_cuda_execute_async(const plfft_plan_t *plan,
                                         const void *d_input, void *d_output,
                                         void *d_workspace, void *stream);
 
+/* Four-step C2C FP32 transform that allocates no device memory.
+ *
+ * No counterpart in the reference.  For callers that must not allocate device
+ * memory while they run: applications whose framework has already reserved
+ * the GPU's memory in its own pool (a cudaMalloc here would fail or fragment
+ * that pool), and latency-critical loops where cudaMalloc/cudaFree would
+ * synchronize the device.  It needs no plan and no workspace.
+ *
+ * Layout: `howmany` contiguous transforms of `n` complex FP32 elements (unit
+ * stride, distance n) at d_input / d_output (device pointers; in place is
+ * allowed); unnormalized, `direction` as in plfft_config_create.  Enqueued on
+ * `stream` (a cudaStream_t, NULL = legacy default stream).
+ *
+ * Limit: 16384 < n <= 2097152 with every prime factor of n in
+ * {2,3,5,7,11,13} and a split n = n1 * n2 with n1, n2 <= 16384; any other n
+ * returns PLFFT_INVALID_SIZE.  The scratch is one file-scope device array of
+ * 17 MiB (16 MiB intermediate buffer + 1 MiB twiddle tables), held on every
+ * GPU that loads the library until the process exits.  The first call on a
+ * device, with that device current, looks up the array's address; make that
+ * first call before any stream capture begins.  Every call rewrites the
+ * parts of the array it reads, and all calls on a device share it, so calls
+ * that overlap on the GPU race and must not be issued. */
+plfft_status_t plfft_cuda_c2c_execute_noalloc(const void *d_input,
+                                             void *d_output, int64_t n,
+                                             int64_t howmany,
+                                             plfft_direction_t direction,
+                                             void *stream);
+
 #ifdef __cplusplus
 }
 #endif

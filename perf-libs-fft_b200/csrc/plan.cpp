@@ -258,12 +258,7 @@ static int tile_threads(int n, const std::vector<int>& radices, int c, int maxe)
   return (need + 31) / 32 * 32;
 }
 
-struct TileChoice {
-  int maxe = 16, c = 1, nthr = 32, ld = 1;
-  std::vector<int> radices;
-};
-
-static bool choose_tile(int64_t n, bool interleaved, TileChoice& tc) {
+bool choose_tile(int64_t n, bool interleaved, TileChoice& tc) {
   if (n > kMaxOnChip || !is_smooth(n)) return false;
   tc.radices = factor_radices(n, 16);
   tc.ld = spad_len(int(n));
@@ -378,15 +373,20 @@ struct C2CFourStepNode : Node {
   }
 };
 
-static std::unique_ptr<Node> make_four_step(int64_t n, const Layout& lay, int dir, float scale,
-                                            std::string* why) {
-  // pick n1 <= n2, both smooth and on chip, n1 as close to sqrt(n) as possible
+int64_t four_step_split(int64_t n) {
+  // n1 <= n2, both smooth and on chip, n1 as close to sqrt(n) as possible
   int64_t best = 0;
   for (int64_t d = 2; d * d <= n; ++d) {
     if (n % d) continue;
     const int64_t e = n / d;
     if (d <= kMaxOnChip && e <= kMaxOnChip && is_smooth(d) && is_smooth(e)) best = d;
   }
+  return best;
+}
+
+static std::unique_ptr<Node> make_four_step(int64_t n, const Layout& lay, int dir, float scale,
+                                            std::string* why) {
+  const int64_t best = four_step_split(n);
   if (!best) {
     if (why) *why = "length " + std::to_string(n) + " has no on-chip four-step split";
     return nullptr;

@@ -104,6 +104,15 @@ void unit_root(int64_t k, int64_t n, double& c, double& s);
 // largest length one CTA transforms on chip
 constexpr int kMaxOnChip = 16384;
 
+// shared-memory tile schedule for length n (c transforms per CTA)
+struct TileChoice {
+  int maxe = 16, c = 1, nthr = 32, ld = 1;
+  std::vector<int> radices;
+};
+bool choose_tile(int64_t n, bool interleaved, TileChoice& tc);
+// four-step split n = n1 * (n / n1) with both factors on chip (0 if none)
+int64_t four_step_split(int64_t n);
+
 // C2C FP32 node for a strided batch (dir -1/+1); scale applied on output.
 std::unique_ptr<Node> make_c2c_node(int64_t n, const Layout& lay, int dir, float scale,
                                     int precision, std::string* why);

@@ -133,6 +133,7 @@ _SIGS = [
     ("plfft_cuda_plan_get_launch_count", _INT, [_P]),
     ("plfft_cuda_plan_describe", _INT, [_P, ctypes.c_char_p, ctypes.c_size_t]),
     ("plfft_cuda_execute_async", _INT, [_P, _P, _P, _P, _P]),
+    ("plfft_cuda_c2c_execute_noalloc", _INT, [_P, _P, _I64, _I64, _INT, _P]),
 ]
 
 # symbols bound when the library exports them (added by later components)
@@ -280,6 +281,14 @@ class Plan:
         buf = ctypes.create_string_buffer(4096)
         _check(lib().plfft_cuda_plan_describe(self.handle, buf, 4096), "describe")
         return buf.value.decode()
+
+
+def c2c_execute_noalloc(d_in, d_out, n, howmany, direction=FORWARD, stream=0):
+    """plfft_cuda_c2c_execute_noalloc: four-step C2C with no device allocation
+    (device pointers, contiguous batch).  Returns the plfft_status_t."""
+    return Status(lib().plfft_cuda_c2c_execute_noalloc(
+        ctypes.c_void_p(int(d_in)), ctypes.c_void_p(int(d_out)), int(n), int(howmany), int(direction),
+        ctypes.c_void_p(int(stream)) if stream else None))
 
 
 def make_plan(kind, n, howmany=1, istride=1, idist=None, ostride=1, odist=None, direction=FORWARD,
