@@ -60,6 +60,22 @@ plfft_status_t plfft_cuda_execute_async(const plfft_plan_t *plan,
                                         const void *d_input, void *d_output,
                                         void *d_workspace, void *stream);
 
+/* Adjoint (transpose for real data, conjugate transpose for complex data) of
+ * the plan's transform, with the plan's scale: d_input uses the plan's OUTPUT
+ * layout and d_output its INPUT layout.  No counterpart in the reference;
+ * this is the backward pass used for differentiation (C2C -> opposite
+ * direction, R2C <-> C2R with Hermitian-fold weights, DCT-II <-> DCT-III,
+ * DST-II <-> DST-III, symmetric kinds self-adjoint).  The adjoint schedule is
+ * built on first use.  `d_workspace` may be NULL (plan-owned buffer). */
+plfft_status_t plfft_cuda_execute_adjoint_async(const plfft_plan_t *plan,
+                                                const void *d_input,
+                                                void *d_output,
+                                                void *d_workspace,
+                                                void *stream);
+plfft_status_t
+plfft_cuda_plan_get_adjoint_workspace_size(const plfft_plan_t *plan,
+                                           size_t *bytes);
+
 /* Four-step C2C FP32 transform that allocates no device memory.
  *
  * No counterpart in the reference.  For callers that must not allocate device

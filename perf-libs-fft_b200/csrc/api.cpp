@@ -237,6 +237,35 @@ plfft_status_t plfft_cuda_execute_async(const plfft_plan_t* plan, const void* in
   return g_last_status;
 }
 
+// builds the adjoint schedule once (plan mutex); returns false on failure
+static bool ensure_adjoint(const PlanData& p) {
+  std::lock_guard<std::mutex> lock(p.mu);
+  if (p.adjoint) return true;
+  std::string why;
+  auto node = make_adjoint_node(p.cfg, &why);
+  if (!node) return false;
+  if (p.adj_ws.alloc(node->workspace()) != cudaSuccess) return false;
+  p.adjoint = std::move(node);
+  return true;
+}
+
+plfft_status_t plfft_cuda_plan_get_adjoint_workspace_size(const plfft_plan_t* plan, size_t* bytes) {
+  if (!plan || !bytes) return PLFFT_NULL_ARGUMENT;
+  if (!ensure_adjoint(plan->p)) return PLFFT_PLAN_CREATION_FAILED;
+  *bytes = plan->p.adjoint->workspace();
+  return PLFFT_OK;
+}
+
+plfft_status_t plfft_cuda_execute_adjoint_async(const plfft_plan_t* plan, const void* in, void* out, void* ws,
+                                                void* stream) {
+  if (!plan || !in || !out) return PLFFT_NULL_ARGUMENT;
+  const PlanData& p = plan->p;
+  if (!ensure_adjoint(p)) return g_last_status = PLFFT_PLAN_CREATION_FAILED;
+  const cudaError_t e = p.adjoint->run(in, out, ws ? ws : p.adj_ws.p, static_cast<cudaStream_t>(stream));
+  g_last_status = from_cuda(e);
+  return g_last_status;
+}
+
 void plfft_plan_execute(const plfft_plan_t* plan, const void* in, void* out) {
   g_last_status = execute_sync(plan->p, in, out);
 }

@@ -89,6 +89,21 @@ enum RealWrapKind {
   RW_R2HC = 11,
   RW_HC2R = 12
 };
+// Elementwise weights that turn a transform into the adjoint of another
+// (input weights applied by the pre-kernel, output weights by the post-kernel)
+enum AdjointWeight {
+  AW_NONE = 0,
+  AW_HERM_HALF = 1,    // complex bins 0 < k < n/2 times 1/2
+  AW_HERM_DOUBLE = 2,  // complex bins 0 < k < n/2 times 2
+  AW_FIRST_X2 = 3,     // element 0 times 2
+  AW_FIRST_HALF = 4,   // element 0 times 1/2
+  AW_LAST_X2 = 5,      // element n-1 times 2
+  AW_LAST_HALF = 6,    // element n-1 times 1/2
+  AW_INNER_HALF = 7,   // elements 0 < j < n-1 times 1/2
+  AW_INNER_X2 = 8,     // elements 0 < j < n-1 times 2
+  AW_HC_HALF = 9,      // half-complex entries other than 0 and n/2 times 1/2
+  AW_HC_DOUBLE = 10    // half-complex entries other than 0 and n/2 times 2
+};
 struct RealWrapLaunch {
   const void* in;
   void* out;
@@ -96,6 +111,7 @@ struct RealWrapLaunch {
   int64_t n, len, nout;
   int64_t istride, idist, ostride, odist;
   float scale;
+  int wmode_in, wmode_out;
 };
 cudaError_t launch_realwrap(bool pre, int kind, const RealWrapLaunch& L, int64_t m0, int64_t cnt,
                             cudaStream_t st);
@@ -124,6 +140,49 @@ struct ConvLaunch {
   float scale;
 };
 cudaError_t launch_conv(int step, const ConvLaunch& L, int64_t m0, int64_t cnt, cudaStream_t st);
+
+// Grouped mixed-length execution (grouped.cu)
+enum GTaskType { GT_TILE = 0, GT_RADER = 1, GT_BLUE = 2 };
+enum GOp {
+  GO_NONE = 0,
+  GO_GATHER = 1,      // prologue: x[perm_in[e]]
+  GO_CHIRP = 2,       // prologue: x[e] * tab[e] (0 for e >= len); epilogue: y * tab[e], e < len only
+  GO_TWIDDLE = 3,     // epilogue: four-step twiddle W^{col * k}
+  GO_SPEC = 4,        // epilogue: y * tab[e]
+  GO_SPEC_SAVE0 = 5,  // epilogue: save y at e == 0, then y * tab[e]
+  GO_SCATTER = 6      // epilogue: out[perm_out[e]] = x0 + y, out[0] = x0 + saved
+};
+constexpr int kGroupBuffers = 3;  // 0 user input, 1 user output, 2 workspace
+struct GTask {
+  int type, dir, n, cnt, desc;
+  int in_buf, out_buf, aux_buf;
+  int pre_op, post_op;
+  int pre_len, post_len;
+  int64_t in_off, out_off, aux_off;
+  int64_t icdist, ikstride, ocdist, okstride;
+  int64_t ie0, iec, iek, oe0, oec, oek;
+  int64_t col0;
+  const float2* pre_tab;
+  const float2* post_tab;
+  const float2* post_tab2;
+  const int* perm_in;
+  const int* perm_out;
+  float2* sum0;
+  TwoLevel tw2;
+  float scale;
+};
+struct GroupPhase {
+  const GTask* tasks;
+  int ntasks;
+  const FftDesc* descs;
+  const float2* const* tws;
+  float2* bases[kGroupBuffers];
+  int* counter;
+  int* done;
+};
+cudaError_t launch_grouped(const GroupPhase& P, int grid, int smem_bytes, cudaStream_t st);
+int grouped_blocks_per_sm(int smem_bytes);
+int group_max_smem_elems();
 
 // kernel entry points (c2c.cu)
 cudaError_t launch_c2c_reg(int e, int dir, const RegLaunch& L, cudaStream_t st);

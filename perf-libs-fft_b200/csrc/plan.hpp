@@ -12,6 +12,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <complex>
 #include <cstdint>
 #include <memory>
 #include <mutex>
@@ -117,13 +118,26 @@ int64_t four_step_split(int64_t n);
 std::unique_ptr<Node> make_c2c_node(int64_t n, const Layout& lay, int dir, float scale,
                                     int precision, std::string* why);
 
+// FP64 host helpers for table generation (plan_conv.cpp)
+using cd = std::complex<double>;
+std::vector<cd> host_fft(const std::vector<cd>& x, int sign);
+std::vector<float2> to_f2(const std::vector<cd>& v, double scale);
+int64_t pow_mod(int64_t a, int64_t e, int64_t p);
+int64_t primitive_root(int64_t p);
+
 // Rader (prime n, smooth n-1) or Bluestein (any n) convolution node.
 std::unique_ptr<Node> make_conv_node(int64_t n, const Layout& lay, int dir, float scale, std::string* why);
 int64_t next_smooth(int64_t n);
 
 // R2C / C2R / R2R through a C2C plan of a related length (realwrap.cu);
 // kind is a RealWrapKind.
-std::unique_ptr<Node> make_realwrap_node(int kind, int64_t n, const Layout& lay, float scale, std::string* why);
+std::unique_ptr<Node> make_realwrap_node(int kind, int64_t n, const Layout& lay, float scale, std::string* why,
+                                         int wmode_in = 0, int wmode_out = 0);
+
+// Adjoint of a plan's transform (same scale, input/output layouts swapped):
+// the conjugate-direction C2C, or the transposed real transform expressed
+// as another kind with elementwise weights.
+std::unique_ptr<Node> make_adjoint_node(const ConfigData& c, std::string* why);
 
 // The plan object behind plfft_plan_t.
 struct PlanData {
@@ -132,6 +146,9 @@ struct PlanData {
   int device = 0;
   DevBuf ws;  // workspace for plfft_plan_execute and *_async without a
               // caller-provided workspace
+  // adjoint schedule, built on the first adjoint execution
+  mutable std::unique_ptr<Node> adjoint;
+  mutable DevBuf adj_ws;
   // host-pointer staging (plfft_plan_execute with host buffers)
   mutable std::mutex mu;
   mutable DevBuf stage_in, stage_out;

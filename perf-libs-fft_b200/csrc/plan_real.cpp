@@ -13,6 +13,7 @@ struct RealWrapNode : Node {
   int64_t n = 0, len = 0, nout = 0;
   Layout lay{};
   float scale = 1.f;
+  int wmode_in = AW_NONE, wmode_out = AW_NONE;
   int64_t chunk = 1;
   std::unique_ptr<Node> inner;  // C2C of length len over `chunk` contiguous members, in place
   size_t inner_ws() const { return inner->workspace(); }
@@ -28,7 +29,8 @@ struct RealWrapNode : Node {
     float2* work = static_cast<float2*>(ws);
     const size_t work_bytes = (size_t(chunk) * size_t(len) * sizeof(float2) + 255) & ~size_t(255);
     void* iws = static_cast<char*>(ws) + work_bytes;
-    RealWrapLaunch L{in, out, work, n, len, nout, lay.istride, lay.idist, lay.ostride, lay.odist, scale};
+    RealWrapLaunch L{in, out, work, n, len, nout, lay.istride, lay.idist, lay.ostride, lay.odist, scale,
+                     wmode_in, wmode_out};
     for (int64_t m0 = 0; m0 < lay.howmany; m0 += chunk) {
       const int64_t cnt = std::min(chunk, lay.howmany - m0);
       cudaError_t e = launch_realwrap(true, kind, L, m0, cnt, st);
@@ -81,7 +83,8 @@ int wrap_dir(int kind) {
 
 }  // namespace
 
-std::unique_ptr<Node> make_realwrap_node(int kind, int64_t n, const Layout& lay, float scale, std::string* why) {
+std::unique_ptr<Node> make_realwrap_node(int kind, int64_t n, const Layout& lay, float scale, std::string* why,
+                                         int wmode_in, int wmode_out) {
   if (kind == RW_DCT1 && n < 2) {
     if (why) *why = "DCT-I needs n > 1";
     return nullptr;
@@ -93,6 +96,8 @@ std::unique_ptr<Node> make_realwrap_node(int kind, int64_t n, const Layout& lay,
   node->nout = kind == RW_R2C ? n / 2 + 1 : n;
   node->lay = lay;
   node->scale = scale;
+  node->wmode_in = wmode_in;
+  node->wmode_out = wmode_out;
   const int64_t target = 64ll << 20;  // bytes of complex work per chunk
   node->chunk = std::max<int64_t>(1, std::min<int64_t>(lay.howmany, target / (node->len * 8)));
   Layout inner{node->chunk, 1, node->len, 1, node->len};

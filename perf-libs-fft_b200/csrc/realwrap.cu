@@ -46,9 +46,27 @@ __device__ __forceinline__ float2 expi_pi(int64_t num, int64_t den) {
   return make_float2(float(c), float(s));
 }
 
+// weight of element j (length n) under an AdjointWeight mode
+__device__ __forceinline__ float adj_weight(int mode, int64_t j, int64_t n) {
+  switch (mode) {
+    case AW_HERM_HALF: return (j > 0 && 2 * j < n) ? 0.5f : 1.f;
+    case AW_HERM_DOUBLE: return (j > 0 && 2 * j < n) ? 2.f : 1.f;
+    case AW_FIRST_X2: return j == 0 ? 2.f : 1.f;
+    case AW_FIRST_HALF: return j == 0 ? 0.5f : 1.f;
+    case AW_LAST_X2: return j == n - 1 ? 2.f : 1.f;
+    case AW_LAST_HALF: return j == n - 1 ? 0.5f : 1.f;
+    case AW_INNER_HALF: return (j > 0 && j < n - 1) ? 0.5f : 1.f;
+    case AW_INNER_X2: return (j > 0 && j < n - 1) ? 2.f : 1.f;
+    case AW_HC_HALF: return (j == 0 || 2 * j == n) ? 1.f : 0.5f;
+    case AW_HC_DOUBLE: return (j == 0 || 2 * j == n) ? 1.f : 2.f;
+    default: return 1.f;
+  }
+}
+
 template <int KIND>
 __device__ __forceinline__ float load_real(const RealWrapLaunch& L, int64_t b, int64_t j) {
-  return static_cast<const float*>(L.in)[b * L.idist + j * L.istride];
+  const float v = static_cast<const float*>(L.in)[b * L.idist + j * L.istride];
+  return L.wmode_in ? v * adj_weight(L.wmode_in, j, L.n) : v;
 }
 
 template <int KIND>
@@ -68,9 +86,11 @@ __global__ void __launch_bounds__(256) realwrap_pre(const RealWrapLaunch L, int6
       if (j <= h) {
         z = X[j * L.istride];
         if (j == 0 || (2 * j == n)) z.y = 0.f;
+        if (L.wmode_in) z = cscale(z, adj_weight(L.wmode_in, j, n));
       } else {
         const float2 c = X[(n - j) * L.istride];
         z = make_float2(c.x, -c.y);
+        if (L.wmode_in) z = cscale(z, adj_weight(L.wmode_in, n - j, n));
       }
     } else if constexpr (KIND == RW_HC2R) {
       const int64_t h = n / 2;
@@ -130,7 +150,8 @@ __global__ void __launch_bounds__(256) realwrap_post(const RealWrapLaunch L, int
     if constexpr (KIND == RW_R2C) {
       float2* Y = static_cast<float2*>(L.out) + b * L.odist;
       const float2 v = F[k];
-      Y[k * L.ostride] = make_float2(v.x * s, v.y * s);
+      const float sw = L.wmode_out ? s * adj_weight(L.wmode_out, k, n) : s;
+      Y[k * L.ostride] = make_float2(v.x * sw, v.y * sw);
     } else {
       float y = 0.f;
       if constexpr (KIND == RW_C2R || KIND == RW_HC2R || KIND == RW_DCT1 || KIND == RW_DCT3) {
@@ -158,7 +179,8 @@ __global__ void __launch_bounds__(256) realwrap_post(const RealWrapLaunch L, int
         else
           y = -2.f * (v.x * w.y + v.y * w.x);
       }
-      static_cast<float*>(L.out)[b * L.odist + k * L.ostride] = y * s;
+      const float sw = L.wmode_out ? s * adj_weight(L.wmode_out, k, n) : s;
+      static_cast<float*>(L.out)[b * L.odist + k * L.ostride] = y * sw;
     }
   }
 }

@@ -134,6 +134,8 @@ _SIGS = [
     ("plfft_cuda_plan_describe", _INT, [_P, ctypes.c_char_p, ctypes.c_size_t]),
     ("plfft_cuda_execute_async", _INT, [_P, _P, _P, _P, _P]),
     ("plfft_cuda_c2c_execute_noalloc", _INT, [_P, _P, _I64, _I64, _INT, _P]),
+    ("plfft_cuda_execute_adjoint_async", _INT, [_P, _P, _P, _P, _P]),
+    ("plfft_cuda_plan_get_adjoint_workspace_size", _INT, [_P, ctypes.POINTER(ctypes.c_size_t)]),
 ]
 
 # symbols bound when the library exports them (added by later components)
@@ -268,6 +270,14 @@ class Plan:
                                             ctypes.c_void_p(int(workspace)) if workspace else None,
                                             ctypes.c_void_p(int(stream)) if stream else None)
         _check(st, "plfft_cuda_execute_async")
+
+    def execute_adjoint(self, inp, out, workspace=0, stream=0):
+        """Adjoint of this plan's transform (input = plan's output layout)."""
+        st = lib().plfft_cuda_execute_adjoint_async(self.handle, ctypes.c_void_p(int(inp)),
+                                                    ctypes.c_void_p(int(out)),
+                                                    ctypes.c_void_p(int(workspace)) if workspace else None,
+                                                    ctypes.c_void_p(int(stream)) if stream else None)
+        _check(st, "plfft_cuda_execute_adjoint_async")
 
     def workspace_size(self):
         v = ctypes.c_size_t()
