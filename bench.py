@@ -1,21 +1,28 @@
 #!/usr/bin/env python3
-"""Benchmark of the batched 1D FFT hot path on B200.
+"""Benchmark of PLFFT's batched 1D transform path on B200.
+
+  python bench.py --gpus N --steps K --warmup W [--impl reference] [--workload NAME]
 
 Default workload (the configuration the headline metric is quoted on):
 plain C2C FP32 forward, N=1024, batch=4096, unit stride, contiguous,
-out-of-place, no scaling; re/im i.i.d. U[-1,1) from a seed.
+out-of-place, no scaling; re/im i.i.d. U[-1,1) from a seed.  Other workloads
+(--workload) cover the remaining configurations: R2C/C2R round trip, DCT-II,
+DST-II, Q0.15, the long C2C lengths, the grouped mixed-length batch and the
+differentiation step.
 
-  python bench.py --gpus N --steps K --warmup W [--impl reference]
+One JSON line on rank 0.  `value` = algorithmic GB/s (one read of every input
+plus one write of every output per step, BASELINE.md definitions) summed over
+ranks, device-timed with CUDA events on the launching stream, max over ranks.
+Inputs rotate over buffer sets totalling more than 4x the 126 MB L2, so no
+step starts L2-warm.  `e2e` is the same metric through the public entry point
+with pinned host buffers (host->device and device->host copies inside the
+timed region).  `--impl reference` times the CPU implementation of the path:
+the FP64 port of the reference's transform definitions in oracle/ (the
+reference itself is AArch64-only and does not build on this x86_64 host),
+on all host cores, on a bounded sample of the same workload.
 
-One JSON line on rank 0.  `value` = algorithmic GB/s (one read of the input
-+ one write of the output per transform) over all ranks, device-timed with
-CUDA events on the launching stream, max over ranks.  Inputs rotate over
-buffer sets whose total size exceeds L2 so no step starts L2-warm.
-`e2e` = the same metric through plfft_plan_execute() on pinned host buffers
-(host->device and device->host copies inside the timed region).
-`--impl reference` times the CPU implementation of the path (the FP64 port
-of the reference's transform definitions, `oracle/`; the reference itself is
-AArch64-only and cannot be built on this x86_64 host).
+Multi-GPU (torchrun, one rank per GPU): every rank runs the full workload on
+its own GPU (batch replicas, weak scaling); there is no data-path collective.
 """
 import argparse
 import json
@@ -30,30 +37,356 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "perf-libs-fft_b200"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
 
-WORKLOADS = {
-    "c2c_n1024_b4096": dict(kind="c2c", n=1024, batch=4096, desc="plain C2C FP32 forward N=1024 batch=4096"),
-}
-
-
-def parse():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=10)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2c_n1024_b4096", choices=list(WORKLOADS))
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    return ap.parse_args()
+L2_BYTES = 126 << 20
 
 
-def algo_bytes(w):
-    n, b = w["n"], w["batch"]
-    if w["kind"] == "c2c":
-        return 2 * n * b * 8
-    raise ValueError(w["kind"])
+# --------------------------------------------------------------------------
+# workloads
+# --------------------------------------------------------------------------
+class Workload:
+    """One step = one pass of the hot path over one batch."""
+
+    name = ""
+    desc = ""
+    dtype = "f32"
+    profile = None  # profiles/<name>.md holding traffic_bytes_per_launch
+
+    def config(self):
+        return {}
 
 
+def _rand_complex(count, gen):
+    import torch
+
+    re_ = torch.rand(count, device="cuda", generator=gen) * 2 - 1
+    im_ = torch.rand(count, device="cuda", generator=gen) * 2 - 1
+    return torch.complex(re_, im_)
+
+
+class PlanWorkload(Workload):
+    """A single plfft plan executed per step."""
+
+    def __init__(self, name, desc, kind, n, batch, r2r=None, precision=0, profile=None):
+        self.name, self.desc, self.kind, self.n, self.batch = name, desc, kind, n, batch
+        self.r2r, self.precision, self.profile = r2r, precision, profile
+
+    def sizes(self):
+        n, b = self.n, self.batch
+        h = n // 2 + 1
+        if self.kind == "c2c":
+            return n * b * 8, n * b * 8
+        if self.kind == "r2c":
+            return n * b * 4, h * b * 8
+        if self.kind == "c2r":
+            return h * b * 8, n * b * 4
+        return n * b * 4, n * b * 4
+
+    def algo_bytes(self):
+        i, o = self.sizes()
+        return i + o
+
+    def flops(self):
+        import math
+
+        f = 5 * self.n * math.log2(max(self.n, 2)) * self.batch
+        return f if self.kind == "c2c" else f / 2
+
+    def config(self):
+        return {"workload": self.desc, "kind": self.kind, "n": self.n, "batch": self.batch,
+                "layout": "unit stride, contiguous, out-of-place",
+                "precision": "split_bf16" if self.precision else "fp32"}
+
+    def setup(self, gen):
+        import torch
+
+        import plfft
+
+        kw = {}
+        if self.kind == "r2r":
+            kw["r2r_kind"] = plfft.R2RKind[self.r2r]
+        self.plan = plfft.make_plan(self.kind, self.n, self.batch, precision=self.precision, **kw)
+        ib, ob = self.sizes()
+        self.sets = max(2, -(-4 * L2_BYTES // (ib + ob)))
+        self.ins = [torch.empty(ib // 4, dtype=torch.float32, device="cuda").uniform_(-1, 1, generator=gen)
+                    for _ in range(self.sets)]
+        self.outs = [torch.empty(ob // 4, dtype=torch.float32, device="cuda") for _ in range(self.sets)]
+        self.ws = torch.empty(max(1, self.plan.workspace_size()), dtype=torch.uint8, device="cuda")
+        self.launches = self.plan.launch_count()
+
+    def step(self, i, stream):
+        self.plan.execute_async(self.ins[i % self.sets].data_ptr(), self.outs[i % self.sets].data_ptr(),
+                                self.ws.data_ptr(), stream)
+
+    def e2e(self, steps):
+        import torch
+
+        ib, ob = self.sizes()
+        hx = self.ins[0].cpu().pin_memory()
+        hy = torch.empty(ob // 4, dtype=torch.float32).pin_memory()
+        self.plan.execute(hx.data_ptr(), hy.data_ptr())
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(torch.cuda.default_stream())
+        for _ in range(steps):
+            self.plan.execute(hx.data_ptr(), hy.data_ptr())
+        e1.record(torch.cuda.default_stream())
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, ib, ob, "plfft_plan_execute(host pinned buffers)"
+
+    def describe(self):
+        return self.plan.describe()
+
+    def cpu_sample(self, threads):
+        """FP64 oracle on a bounded sample; returns (seconds per sample, sample bytes, text)."""
+        import numpy as np
+
+        import oracle
+
+        per = self.n * 16
+        m = max(1, min(self.batch, int(2e6 // max(1, self.n * max(1, np.log2(self.n))))))
+        if self.kind == "r2r":
+            m = max(1, min(self.batch, int(4e7 // (self.n * self.n))))
+        rng = np.random.default_rng(0)
+        if self.kind == "c2c":
+            x = rng.uniform(-1, 1, (m, self.n)) + 1j * rng.uniform(-1, 1, (m, self.n))
+            fn = lambda: oracle.c2c(x, -1, method="fft", threads=threads)  # noqa: E731
+        elif self.kind in ("r2c", "c2r"):
+            x = rng.uniform(-1, 1, (m, self.n))
+            fn = lambda: oracle.c2r(oracle.r2c(x, method="fft", threads=threads), self.n,  # noqa: E731
+                                    method="fft", threads=threads)
+        elif self.r2r in ("DCT_2", "DST_2"):
+            # FP64 FFT of the length-2N even / odd extension, then the
+            # post-rotation (the same mapping as the device path)
+            m = max(1, min(self.batch, int(2e6 // max(1, 2 * self.n * np.log2(2 * self.n)))))
+            x = rng.uniform(-1, 1, (m, self.n))
+            k = np.arange(self.n)
+            sign = 1.0 if self.r2r == "DCT_2" else -1.0
+
+            def fn():
+                ext = np.concatenate([x, sign * x[:, ::-1]], axis=1).astype(np.complex128)
+                F = oracle.c2c(ext, -1, method="fft", threads=threads)
+                if self.r2r == "DCT_2":
+                    return (np.exp(-1j * np.pi * k / (2 * self.n)) * F[:, : self.n]).real
+                return -(np.exp(-1j * np.pi * (k + 1) / (2 * self.n)) * F[:, 1: self.n + 1]).imag
+        else:
+            x = rng.uniform(-1, 1, (m, self.n))
+            fn = lambda: oracle.r2r(x, self.r2r, threads=threads)  # noqa: E731
+        fn()
+        reps = 3
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        dt = (time.perf_counter() - t0) / reps
+        frac = m / self.batch
+        how = "direct sums" if (self.kind == "r2r" and self.r2r not in ("DCT_2", "DST_2")) else "mixed-radix FFT"
+        return dt, self.algo_bytes() * frac, f"{m} of {self.batch} transforms, FP64 {how} (oracle/)"
+
+
+class RoundTripWorkload(PlanWorkload):
+    """R2C forward then C2R with 1/N scale (one step = both)."""
+
+    def __init__(self, name, desc, n, batch, profile=None):
+        super().__init__(name, desc, "r2c", n, batch, profile=profile)
+
+    def algo_bytes(self):
+        n, b = self.n, self.batch
+        return 2 * (n * b * 4 + (n // 2 + 1) * b * 8)
+
+    def flops(self):
+        import math
+
+        return 5 * self.n * math.log2(self.n) * self.batch
+
+    def config(self):
+        c = super().config()
+        c["kind"] = "r2c + c2r (1/N)"
+        return c
+
+    def setup(self, gen):
+        import torch
+
+        import plfft
+
+        n, b = self.n, self.batch
+        self.plan = plfft.make_plan("r2c", n, b)
+        self.inv = plfft.make_plan("c2r", n, b, scale=1.0 / n)
+        rb, cb = n * b * 4, (n // 2 + 1) * b * 8
+        self.sets = max(2, -(-4 * L2_BYTES // (2 * rb + cb)))
+        self.ins = [torch.empty(rb // 4, device="cuda").uniform_(-1, 1, generator=gen) for _ in range(self.sets)]
+        self.mid = [torch.empty(cb // 4, device="cuda") for _ in range(self.sets)]
+        self.outs = [torch.empty(rb // 4, device="cuda") for _ in range(self.sets)]
+        self.ws = torch.empty(max(1, self.plan.workspace_size(), self.inv.workspace_size()), dtype=torch.uint8,
+                              device="cuda")
+        self.launches = self.plan.launch_count() + self.inv.launch_count()
+
+    def step(self, i, stream):
+        k = i % self.sets
+        self.plan.execute_async(self.ins[k].data_ptr(), self.mid[k].data_ptr(), self.ws.data_ptr(), stream)
+        self.inv.execute_async(self.mid[k].data_ptr(), self.outs[k].data_ptr(), self.ws.data_ptr(), stream)
+
+    def e2e(self, steps):
+        import torch
+
+        n, b = self.n, self.batch
+        hx = self.ins[0].cpu().pin_memory()
+        hy = torch.empty(n * b, dtype=torch.float32).pin_memory()
+        dmid = self.mid[0]
+
+        def one():
+            self.plan.execute(hx.data_ptr(), dmid.data_ptr())
+            self.inv.execute(dmid.data_ptr(), hy.data_ptr())
+
+        one()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(torch.cuda.default_stream())
+        for _ in range(steps):
+            one()
+        e1.record(torch.cuda.default_stream())
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, n * b * 4, n * b * 4, "plfft_plan_execute x2 (host pinned in/out)"
+
+    def describe(self):
+        return self.plan.describe() + " + " + self.inv.describe()
+
+
+class GroupedWorkload(Workload):
+    name = "grouped_4000"
+    desc = ("grouped C2C FP32: 4000 transforms, log-uniform 16..65536 (60% pow2, 20% 2^a3^b5^c7^d, "
+            "10% Rader primes, 10% Bluestein)")
+    profile = None
+
+    def __init__(self, count=4000):
+        import numpy as np
+
+        from helpers import grouped_lengths
+
+        self.count = count
+        L = np.array(sorted(grouped_lengths(self.count, seed=2026)), np.int64)
+        self.lengths = L
+        self.offs = np.concatenate([[0], np.cumsum(L)[:-1]]).astype(np.int64)
+        self.total = int(L.sum())
+
+    def setup(self, gen):
+        import torch
+
+        import plfft
+
+        L = self.lengths
+        self.group = plfft.Group(L, self.offs, self.offs, plfft.FORWARD)
+        self.sets = max(2, -(-4 * L2_BYTES // (16 * self.total)))
+        self.ins = [_rand_complex(self.total, gen) for _ in range(self.sets)]
+        self.outs = [torch.empty(self.total, dtype=torch.complex64, device="cuda") for _ in range(self.sets)]
+        self.launches = self.group.launch_count()
+
+    def algo_bytes(self):
+        return 16 * self.total
+
+    def flops(self):
+        import numpy as np
+
+        return float(np.sum(5 * self.lengths * np.log2(self.lengths)))
+
+    def config(self):
+        import numpy as np
+
+        return {"workload": self.desc, "count": self.count, "distinct_lengths": int(len(np.unique(self.lengths))),
+                "total_elements": self.total, "layout": "transforms contiguous, sorted by length"}
+
+    def step(self, i, stream):
+        k = i % self.sets
+        self.group.execute_async(self.ins[k].data_ptr(), self.outs[k].data_ptr(), stream)
+
+    def e2e(self, steps):
+        import torch
+
+        hx = self.ins[0].cpu().pin_memory()
+        hy = torch.empty(self.total, dtype=torch.complex64).pin_memory()
+        s = torch.cuda.current_stream()
+
+        def one():
+            self.ins[0].copy_(hx, non_blocking=True)
+            self.group.execute_async(self.ins[0].data_ptr(), self.outs[0].data_ptr(), s.cuda_stream)
+            hy.copy_(self.outs[0], non_blocking=True)
+
+        one()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(steps):
+            one()
+        e1.record(s)
+        torch.cuda.synchronize()
+        return (e0.elapsed_time(e1) / steps, 8 * self.total, 8 * self.total,
+                "H2D + plfft_cuda_group_execute_async + D2H (pinned)")
+
+    def describe(self):
+        return self.group.describe()
+
+    def cpu_sample(self, threads):
+        import numpy as np
+
+        import oracle
+
+        pick = self.lengths[:: max(1, len(self.lengths) // 200)]
+        xs = [np.random.default_rng(int(n)).standard_normal(n) + 0j for n in pick]
+        t0 = time.perf_counter()
+        for x in xs:
+            oracle.c2c(x[None], -1, method="fft", threads=threads)
+        dt = time.perf_counter() - t0
+        return dt, 16 * float(np.sum(pick)), f"{len(pick)} of {self.count} transforms, FP64 FFT (oracle/)"
+
+
+class AdjointWorkload(PlanWorkload):
+    """Differentiation step: R2C forward + adjoint (C2R with Hermitian-fold
+    weights) of the weighted power loss, x FP32 1024 x 8192."""
+
+    def __init__(self):
+        super().__init__("diff_r2c_n8192_b1024", "loss = sum W |R2C(x)|^2 forward + adjoint, N=8192 batch=1024",
+                         "r2c", 8192, 1024)
+
+    def algo_bytes(self):
+        n, b = self.n, self.batch
+        return 2 * (n * b * 4 + (n // 2 + 1) * b * 8)
+
+    def step(self, i, stream):
+        k = i % self.sets
+        self.plan.execute_async(self.ins[k].data_ptr(), self.outs[k].data_ptr(), self.ws.data_ptr(), stream)
+        self.plan.execute_adjoint(self.outs[k].data_ptr(), self.ins[(k + 1) % self.sets].data_ptr(), 0, stream)
+
+    def setup(self, gen):
+        super().setup(gen)
+        self.launches *= 2
+
+
+def make_workload(name):
+    table = {
+        "c2c_n1024_b4096": lambda: PlanWorkload("c2c_n1024_b4096", "plain C2C FP32 forward N=1024 batch=4096",
+                                                "c2c", 1024, 4096, profile="c2c_pow2_n1024_b4096"),
+        "r2c_c2r_n4096_b8192": lambda: RoundTripWorkload("r2c_c2r_n4096_b8192",
+                                                         "R2C + C2R(1/N) FP32 round trip N=4096 batch=8192",
+                                                         4096, 8192),
+        "dct2_n1024_b4096": lambda: PlanWorkload("dct2_n1024_b4096", "R2R DCT-II FP32 N=1024 batch=4096", "r2r",
+                                                 1024, 4096, r2r="DCT_2"),
+        "dst2_n1024_b4096": lambda: PlanWorkload("dst2_n1024_b4096", "R2R DST-II FP32 N=1024 batch=4096", "r2r",
+                                                 1024, 4096, r2r="DST_2"),
+        "c2c_n1m_b64": lambda: PlanWorkload("c2c_n1m_b64", "C2C FP32 N=2^20 batch=64", "c2c", 1 << 20, 64),
+        "c2c_n64k_b1024": lambda: PlanWorkload("c2c_n64k_b1024", "C2C FP32 N=2^16 batch=1024", "c2c", 1 << 16, 1024),
+        "grouped_4000": lambda: GroupedWorkload(),
+        "diff_r2c_n8192_b1024": lambda: AdjointWorkload(),
+    }
+    return table[name]()
+
+
+WORKLOAD_NAMES = ["c2c_n1024_b4096", "r2c_c2r_n4096_b8192", "dct2_n1024_b4096", "dst2_n1024_b4096", "c2c_n1m_b64",
+                  "c2c_n64k_b1024", "grouped_4000", "diff_r2c_n8192_b1024"]
+
+
+# --------------------------------------------------------------------------
+# measurement helpers
+# --------------------------------------------------------------------------
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -63,7 +396,9 @@ def peaks():
 
 
 def profile_traffic(name):
-    """dram bytes per launch from the committed ncu summary, or None."""
+    """dram bytes per launch of the dominant kernel from the committed ncu summary."""
+    if not name:
+        return None
     path = os.path.join(ROOT, "profiles", name + ".md")
     if not os.path.exists(path):
         return None
@@ -122,64 +457,51 @@ class ClockSampler:
                     reasons.add(nm)
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference(w, steps, warmup, sample_transforms):
-    """Time the FP64 CPU port (oracle) on a bounded sample of the workload."""
-    import numpy as np
-
+def cpu_baseline(w):
     import oracle
 
     threads = oracle.max_threads()
-    n = w["n"]
-    rng = np.random.default_rng(0)
-    x = rng.uniform(-1, 1, (sample_transforms, n)) + 1j * rng.uniform(-1, 1, (sample_transforms, n))
-    for _ in range(warmup):
-        oracle.c2c(x, -1, method="fft", threads=threads)
-    times = []
-    for _ in range(steps):
-        t0 = time.perf_counter()
-        oracle.c2c(x, -1, method="fft", threads=threads)
-        times.append(time.perf_counter() - t0)
-    per_step = sum(times) / len(times)
-    gbs = 2 * n * sample_transforms * 8 / per_step / 1e9
-    return gbs, threads, per_step
+    dt, sbytes, text = w.cpu_sample(threads)
+    return {"value": sbytes / dt / 1e9, "unit": "GB/s", "cores": threads, "kind": "port", "sample": text}
+
+
+# --------------------------------------------------------------------------
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2c_n1024_b4096", choices=WORKLOAD_NAMES)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
 
 
 def main():
     args = parse()
-    w = WORKLOADS[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    n, batch = w["n"], w["batch"]
-    config = {"workload": w["desc"], "n": n, "batch": batch, "layout": "unit stride, contiguous, out-of-place",
-              "l2": "inputs rotate over buffer sets totalling > 4x L2", "parallelism": f"batch-replica x{args.gpus}"}
+    w = make_workload(args.workload)
 
     if args.impl == "reference":
         if rank != 0:
             return
-        sample = 256
-        gbs, threads, per_step = cpu_reference(w, max(1, min(args.steps, 20)), min(args.warmup, 3), sample)
-        line = {"metric": "batched C2C FP32 GB/s (algorithmic bytes)", "value": gbs, "unit": "GB/s",
-                "impl": "reference", "n_gpus": args.gpus, "steps": max(1, min(args.steps, 20)),
-                "warmup": min(args.warmup, 3), "ms_per_step": per_step * 1e3, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded U[-1,1))",
-                "config": config,
-                "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
-                                 "sample": f"{sample} of {batch} transforms per step, FP64 mixed-radix FFT port of "
-                                           "the reference conventions (the reference is AArch64-only and does not "
-                                           "build on this x86_64 host)"},
-                "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        cpu = cpu_baseline(w)
+        line = {"metric": f"{w.name} GB/s (algorithmic bytes)", "value": cpu["value"], "unit": "GB/s",
+                "impl": "reference", "n_gpus": args.gpus, "steps": 1, "warmup": 1,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded U[-1,1))", "config": w.config(), "cpu_baseline": cpu,
+                "e2e": {"value": cpu["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
 
     import numpy as np
     import torch
-
-    import plfft
 
     torch.cuda.set_device(local)
     dist = None
@@ -195,103 +517,79 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    plan = plfft.make_plan("c2c", n, batch, direction=plfft.FORWARD)
-    launches = plan.launch_count()
-    abytes = algo_bytes(w)
-    l2 = 126 << 20
-    sets = max(2, int(np.ceil(4 * l2 / abytes)))
-    g = torch.Generator(device="cuda")
-    g.manual_seed(1234 + rank)
-    ins, outs = [], []
-    for _ in range(sets):
-        re_ = torch.rand(batch * n, device="cuda", generator=g) * 2 - 1
-        im_ = torch.rand(batch * n, device="cuda", generator=g) * 2 - 1
-        ins.append(torch.complex(re_, im_))
-        outs.append(torch.empty(batch * n, dtype=torch.complex64, device="cuda"))
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(1234 + rank)
+    w.setup(gen)
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
-    ws = torch.empty(max(1, plan.workspace_size()), dtype=torch.uint8, device="cuda")
 
     sampler = ClockSampler(local)
     sampler.start()
     for i in range(args.warmup):
-        plan.execute_async(ins[i % sets].data_ptr(), outs[i % sets].data_ptr(), ws.data_ptr(), sh)
+        w.step(i, sh)
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for i in range(args.steps):
-        plan.execute_async(ins[i % sets].data_ptr(), outs[i % sets].data_ptr(), ws.data_ptr(), sh)
+        w.step(i, sh)
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier()
     ms = ev0.elapsed_time(ev1)
-    # per-launch duration of the dominant kernel (one launch per step here)
-    kev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * min(args.steps, 50))]
-    for i in range(len(kev) // 2):
+    # per-step device time (each step bracketed by events)
+    nk = min(args.steps, 50)
+    kev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * nk)]
+    for i in range(nk):
         kev[2 * i].record(stream)
-        plan.execute_async(ins[i % sets].data_ptr(), outs[i % sets].data_ptr(), ws.data_ptr(), sh)
+        w.step(i, sh)
         kev[2 * i + 1].record(stream)
     torch.cuda.synchronize()
-    kms = [kev[2 * i].elapsed_time(kev[2 * i + 1]) for i in range(len(kev) // 2)]
-    kernel_ms = statistics.median(kms) / launches
-
-    # end to end through the public API on pinned host buffers
-    hx = ins[0].cpu().pin_memory()
-    hy = torch.empty(batch * n, dtype=torch.complex64).pin_memory()
-    plan.execute(hx.data_ptr(), hy.data_ptr())  # warm the staging buffers
-    e2e_steps = max(3, min(args.steps, 20))
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(torch.cuda.default_stream())
-    for _ in range(e2e_steps):
-        plan.execute(hx.data_ptr(), hy.data_ptr())
-    e1.record(torch.cuda.default_stream())
-    torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    step_ms = statistics.median(kev[2 * i].elapsed_time(kev[2 * i + 1]) for i in range(nk))
+    e2e = None
+    if not args.no_e2e:
+        e2e_ms, hb, db, api = w.e2e(max(3, min(args.steps, 20)))
+        e2e = {"value": w.algo_bytes() * world / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s",
+               "h2d_bytes_per_step": hb, "d2h_bytes_per_step": db, "ms_per_step": e2e_ms, "api": api}
     clocks = sampler.stop()
 
     if dist is not None:
-        t = torch.tensor([ms, e2e_ms, kernel_ms], device="cuda")
+        t = torch.tensor([ms, step_ms, e2e["ms_per_step"] if e2e else 0.0], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms, kernel_ms = [float(v) for v in t.tolist()]
+        ms, step_ms, e2e_max = [float(v) for v in t.tolist()]
+        if e2e:
+            e2e["ms_per_step"] = e2e_max
+            e2e["value"] = w.algo_bytes() * world / (e2e_max * 1e-3) / 1e9
 
     ms_per_step = ms / args.steps
+    abytes = w.algo_bytes()
     value = abytes * world / (ms_per_step * 1e-3) / 1e9
     peak, peak_kind = peaks()
-    achieved = abytes / launches / (kernel_ms * 1e-3) / 1e9
-    traffic = profile_traffic("c2c_reg_n1024_b4096")
-
+    achieved = abytes / (step_ms * 1e-3) / 1e9
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        sample = 256
-        gbs, threads, _ = cpu_reference(w, 10, 2, sample)
-        cpu = {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "port",
-               "sample": f"{sample} of {batch} transforms, FP64 mixed-radix FFT port (oracle/), 10 timed reps"}
-
+        cpu = cpu_baseline(w)
     if rank == 0:
         line = {
-            "metric": "batched C2C FP32 GB/s (algorithmic bytes)", "value": value, "unit": "GB/s",
+            "metric": f"{w.name} GB/s (algorithmic bytes)", "value": value, "unit": "GB/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded U[-1,1) re/im)", "config": config,
-            "gflops": 5 * n * np.log2(n) * batch * world / (ms_per_step * 1e-3) / 1e9,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": w.dtype,
+            "data": "synthetic (seeded U[-1,1) re/im)",
+            "config": dict(w.config(), l2="inputs rotate over buffer sets totalling > 4x L2",
+                           parallelism=f"batch replicas x{world}, no collective"),
+            "gflops": w.flops() * world / (ms_per_step * 1e-3) / 1e9,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
-                         "kernel_ms": kernel_ms, "algorithmic_bytes_per_launch": abytes // launches},
-            "e2e": {"value": abytes * world / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s",
-                    "h2d_bytes_per_step": batch * n * 8, "d2h_bytes_per_step": batch * n * 8,
-                    "ms_per_step": e2e_ms, "api": "plfft_plan_execute(host pinned buffers)"},
-            "gpu_launches": launches * args.steps,
-            "plan": plan.describe(),
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": profile_traffic(w.profile), "kernel_ms": step_ms,
+                         "algorithmic_bytes_per_step": abytes, "launches_per_step": w.launches},
+            "e2e": e2e,
+            "gpu_launches": w.launches * args.steps,
+            "plan": w.describe(),
             "clocks": clocks,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))
-    plan.destroy()
     if dist is not None:
         dist.destroy_process_group()
 

@@ -76,6 +76,28 @@ plfft_status_t
 plfft_cuda_plan_get_adjoint_workspace_size(const plfft_plan_t *plan,
                                            size_t *bytes);
 
+/* Grouped execution of many C2C FP32 transforms of different lengths.
+ * No counterpart in the reference (a PLFFT user creates one plan per length).
+ * Transform i has lengths[i] contiguous complex elements starting at element
+ * in_offsets[i] of the input buffer and out_offsets[i] of the output buffer
+ * (the output regions must not overlap each other or any input region).
+ * Every length is accepted: on-chip lengths, Rader primes, Bluestein lengths
+ * and four-step lengths all run inside the same persistent kernel, at most
+ * four launches (one per dependency phase) replayed as one CUDA graph. */
+typedef struct plfft_cuda_group_t plfft_cuda_group_t;
+plfft_status_t plfft_cuda_group_create(plfft_cuda_group_t **group,
+                                       int64_t count, const int64_t *lengths,
+                                       const int64_t *in_offsets,
+                                       const int64_t *out_offsets,
+                                       plfft_direction_t direction);
+plfft_status_t plfft_cuda_group_execute_async(plfft_cuda_group_t *group,
+                                              const void *d_input,
+                                              void *d_output, void *stream);
+int plfft_cuda_group_get_launch_count(const plfft_cuda_group_t *group);
+plfft_status_t plfft_cuda_group_describe(const plfft_cuda_group_t *group,
+                                         char *buf, size_t len);
+void plfft_cuda_group_destroy(plfft_cuda_group_t *group);
+
 /* Four-step C2C FP32 transform that allocates no device memory.
  *
  * No counterpart in the reference.  For callers that must not allocate device

@@ -16,7 +16,6 @@
 
 namespace plfft_b200 {
 
-using cd = std::complex<double>;
 
 // FP64 host FFT for smooth lengths (tables only): recursive decimation in
 // time, each prime factor by a direct DFT, twiddles from an exact-index root
@@ -44,7 +43,7 @@ static void host_fft_rec(const cd* x, int64_t xs, cd* y, int64_t n, int sign, co
   }
 }
 
-static std::vector<cd> host_fft(const std::vector<cd>& x, int sign) {
+std::vector<cd> host_fft(const std::vector<cd>& x, int sign) {
   const int64_t n = int64_t(x.size());
   std::vector<cd> w(n), y(n);
   for (int64_t k = 0; k < n; ++k) {
@@ -57,13 +56,13 @@ static std::vector<cd> host_fft(const std::vector<cd>& x, int sign) {
   return y;
 }
 
-static std::vector<float2> to_f2(const std::vector<cd>& v, double scale = 1.0) {
+std::vector<float2> to_f2(const std::vector<cd>& v, double scale) {
   std::vector<float2> r(v.size());
   for (size_t i = 0; i < v.size(); ++i) r[i] = make_float2(float(v[i].real() * scale), float(v[i].imag() * scale));
   return r;
 }
 
-static int64_t pow_mod(int64_t a, int64_t e, int64_t p) {
+int64_t pow_mod(int64_t a, int64_t e, int64_t p) {
   __int128 r = 1, b = a % p;
   while (e) {
     if (e & 1) r = (r * b) % p;
@@ -74,7 +73,7 @@ static int64_t pow_mod(int64_t a, int64_t e, int64_t p) {
 }
 
 // smallest primitive root of prime p: g^((p-1)/q) != 1 for every prime q | p-1
-static int64_t primitive_root(int64_t p) {
+int64_t primitive_root(int64_t p) {
   std::vector<int64_t> qs;
   int64_t m = p - 1;
   for (int64_t q = 2; q * q <= m; ++q)
@@ -213,7 +212,7 @@ std::unique_ptr<Node> make_conv_node(int64_t n, const Layout& lay, int dir, floa
       b[k] = std::conj(w[k]);
       if (k) b[m - k] = std::conj(w[k]);
     }
-    if (node->chirp.upload(to_f2(w)) != cudaSuccess) {
+    if (node->chirp.upload(to_f2(w, 1.0)) != cudaSuccess) {
       if (why) *why = "device allocation failed";
       return nullptr;
     }

@@ -136,6 +136,11 @@ _SIGS = [
     ("plfft_cuda_c2c_execute_noalloc", _INT, [_P, _P, _I64, _I64, _INT, _P]),
     ("plfft_cuda_execute_adjoint_async", _INT, [_P, _P, _P, _P, _P]),
     ("plfft_cuda_plan_get_adjoint_workspace_size", _INT, [_P, ctypes.POINTER(ctypes.c_size_t)]),
+    ("plfft_cuda_group_create", _INT, [_PP, _I64, _P, _P, _P, _INT]),
+    ("plfft_cuda_group_execute_async", _INT, [_P, _P, _P, _P]),
+    ("plfft_cuda_group_get_launch_count", _INT, [_P]),
+    ("plfft_cuda_group_describe", _INT, [_P, ctypes.c_char_p, ctypes.c_size_t]),
+    ("plfft_cuda_group_destroy", None, [_P]),
 ]
 
 # symbols bound when the library exports them (added by later components)
@@ -299,6 +304,47 @@ def c2c_execute_noalloc(d_in, d_out, n, howmany, direction=FORWARD, stream=0):
     return Status(lib().plfft_cuda_c2c_execute_noalloc(
         ctypes.c_void_p(int(d_in)), ctypes.c_void_p(int(d_out)), int(n), int(howmany), int(direction),
         ctypes.c_void_p(int(stream)) if stream else None))
+
+
+class Group:
+    """plfft_cuda_group_t: many C2C transforms of different lengths in one grouped execution."""
+
+    def __init__(self, lengths, in_offsets, out_offsets, direction=FORWARD):
+        import numpy as np
+
+        self._len = np.ascontiguousarray(lengths, dtype=np.int64)
+        self._io = np.ascontiguousarray(in_offsets, dtype=np.int64)
+        self._oo = np.ascontiguousarray(out_offsets, dtype=np.int64)
+        h = ctypes.c_void_p()
+        st = lib().plfft_cuda_group_create(ctypes.byref(h), len(self._len), self._len.ctypes.data,
+                                           self._io.ctypes.data, self._oo.ctypes.data, int(direction))
+        _check(st, "plfft_cuda_group_create")
+        self.handle = h
+
+    def execute_async(self, d_in, d_out, stream=0):
+        st = lib().plfft_cuda_group_execute_async(self.handle, ctypes.c_void_p(int(d_in)),
+                                                  ctypes.c_void_p(int(d_out)),
+                                                  ctypes.c_void_p(int(stream)) if stream else None)
+        _check(st, "plfft_cuda_group_execute_async")
+
+    def launch_count(self):
+        return lib().plfft_cuda_group_get_launch_count(self.handle)
+
+    def describe(self):
+        buf = ctypes.create_string_buffer(4096)
+        _check(lib().plfft_cuda_group_describe(self.handle, buf, 4096), "group describe")
+        return buf.value.decode()
+
+    def destroy(self):
+        if self.handle is not None:
+            lib().plfft_cuda_group_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
 
 
 def make_plan(kind, n, howmany=1, istride=1, idist=None, ostride=1, odist=None, direction=FORWARD,

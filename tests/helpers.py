@@ -63,3 +63,57 @@ def c2c_case(n, howmany=1, istride=1, idist=None, ostride=1, odist=None, directi
     ref = oracle.c2c(xl.astype(np.complex128), direction, method=method) * scale
     got = gather(got_buf, howmany, odist, n, ostride)
     return got, ref, plan
+
+
+def _is_prime(n):
+    if n < 2:
+        return False
+    d = 2
+    while d * d <= n:
+        if n % d == 0:
+            return False
+        d += 1
+    return True
+
+
+def _smooth7(n):
+    for p in (2, 3, 5, 7):
+        while n % p == 0:
+            n //= p
+    return n == 1
+
+
+def grouped_lengths(count, seed=0, min_len=16, max_len=65536):
+    """Seeded lengths for the grouped workload: log-uniform in [min_len, max_len],
+    60% powers of two, 20% 2^a 3^b 5^c 7^d, 10% primes with smooth p-1 (Rader),
+    10% lengths with a large prime factor (Bluestein)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    lo, hi = np.log(min_len), np.log(max_len)
+    while len(out) < count:
+        cls = rng.choice(4, p=[0.6, 0.2, 0.1, 0.1])
+        target = int(np.exp(rng.uniform(lo, hi)))
+        if cls == 0:
+            n = 1 << int(round(np.log2(max(target, 1))))
+        elif cls == 1:
+            n = target
+            while not _smooth7(n):
+                n += 1
+        elif cls == 2:
+            n = target | 1
+            while not (_is_prime(n) and _smooth7_13(n - 1)):
+                n += 2
+        else:
+            n = target
+            while _smooth7_13(n) or _is_prime(n):
+                n += 1
+        if min_len <= n <= max_len:
+            out.append(int(n))
+    return out
+
+
+def _smooth7_13(n):
+    for p in (2, 3, 5, 7, 11, 13):
+        while n % p == 0:
+            n //= p
+    return n == 1
