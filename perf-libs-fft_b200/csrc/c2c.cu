@@ -128,7 +128,7 @@ int tile_smem_bytes(int ld, int c) { return ld * c * int(sizeof(float2)); }
 
 template <class K>
 static cudaError_t set_smem(K kernel, int bytes) {
-  if (bytes > 48 * 1024) {
+  if (bytes > 32 * 1024) {  // leave room for static shared memory
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   }
   return cudaSuccess;

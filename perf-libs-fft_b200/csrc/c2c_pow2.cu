@@ -437,7 +437,7 @@ static cudaError_t run_pow2(const Pow2Launch& L, cudaStream_t st) {
   if (L.tma_in && L.tma_out && L.ring) {
     auto* k = c2c_pow2_ring_kernel<N, E, DIR>;
     const int smem = kRing * pow2_smem_bytes(N, L.g);
-    if (smem > 48 * 1024) {
+    if (smem > 32 * 1024) {  // leave room for static shared memory
       cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
       if (e != cudaSuccess) return e;
     }
@@ -453,7 +453,7 @@ static cudaError_t run_pow2(const Pow2Launch& L, cudaStream_t st) {
     return cudaGetLastError();
   }
   const int smem = pow2_smem_bytes(N, L.g);
-  if (smem > 48 * 1024) {
+  if (smem > 32 * 1024) {  // leave room for static shared memory
     cudaError_t e = cudaFuncSetAttribute(c2c_pow2_kernel<N, E, DIR>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;

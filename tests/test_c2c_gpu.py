@@ -52,7 +52,7 @@ def test_c2c_reference_conv_layouts(case, direction):
     assert oracle.rel_l2(got, ref) <= oracle.fp32_tol(n), plan.describe()
 
 
-@pytest.mark.parametrize("n", [17, 23, 97, 1009, 4099, 1031, 1058, 2 * 8191, 65537, 8191 * 3])
+@pytest.mark.parametrize("n", [17, 23, 97, 1009, 4099, 1031, 1058, 2870, 2 * 8191, 65537, 8191 * 3])
 @pytest.mark.parametrize("direction", [-1, 1])
 def test_c2c_rader_bluestein(n, direction):
     howmany = 3
