@@ -14,87 +14,12 @@
 // twiddle levels; here all levels of one transform stay on chip).
 #include "kernels.h"
 #include "ptx.cuh"
-#include "stockham.cuh"
+#include "pow2_stages.cuh"
 
 #include <algorithm>
 
 namespace plfft_b200 {
 
-template <int N, int E>
-struct P2 {
-  static constexpr int count_e(int m) { return (m % E == 0 && m > 1) ? 1 + count_e(m / E) : 0; }
-  static constexpr int pow_e(int k) { return k == 0 ? 1 : E * pow_e(k - 1); }
-  static constexpr int KE = count_e(N);           // number of full radix-E stages
-  static constexpr int REST = N / pow_e(KE);      // leftover factor (1 or < E)
-  static constexpr int S = KE + (REST > 1 ? 1 : 0);
-  static constexpr int R0 = REST > 1 ? REST : E;
-  static constexpr int T = N / E;
-  static constexpr int radix(int s) { return s == 0 ? R0 : E; }
-  static constexpr int ns(int s) { return s == 0 ? 1 : R0 * pow_e(s - 1); }
-  static constexpr int twoff(int s) { return s <= 1 ? 0 : twoff(s - 1) + (E - 1) * ns(s - 1); }
-};
-
-// TWS: the twiddle table lives in shared memory (plain loads) instead of
-// global memory (read-only cache loads)
-template <int T, int E, int R, int NS, int TWOFF, int DIR, bool TWS = false>
-__device__ __forceinline__ void st_bfly(float2 (&v)[E], int t, const float2* __restrict__ tw) {
-  constexpr int M = E / R;
-#pragma unroll
-  for (int m = 0; m < M; ++m) {
-    float2 x[R];
-#pragma unroll
-    for (int i = 0; i < R; ++i) x[i] = v[m + M * i];
-    if constexpr (NS > 1) {
-      const int j = t + T * m;
-      const int r = j & (NS - 1);
-      const float2* w = tw + TWOFF + r;
-#pragma unroll
-      for (int i = 1; i < R; ++i) {
-        float2 wi;
-        if constexpr (TWS)
-          wi = w[(i - 1) * NS];
-        else
-          wi = __ldg(w + (i - 1) * NS);
-        x[i] = twmul<DIR>(x[i], wi);
-      }
-    }
-    dft<R, DIR>(x);
-#pragma unroll
-    for (int i = 0; i < R; ++i) v[m + M * i] = x[i];
-  }
-}
-
-template <int T, int E, int R, int NS>
-__device__ __forceinline__ void st_scatter(const float2 (&v)[E], int t, float2* sm) {
-  constexpr int M = E / R;
-#pragma unroll
-  for (int m = 0; m < M; ++m) {
-    const int j = t + T * m;
-    const int base = (j & ~(NS - 1)) * R + (j & (NS - 1));
-#pragma unroll
-    for (int i = 0; i < R; ++i) sm[spad(base + i * NS)] = v[m + M * i];
-  }
-}
-
-template <int N, int E, int DIR, int S, bool TWS = false>
-struct Stages {
-  using P = P2<N, E>;
-  template <class Sync>
-  __device__ __forceinline__ static void run(float2 (&v)[E], int t, float2* xb, const float2* tw, Sync sync) {
-    if constexpr (S < P::S) {
-      sync();  // the buffer's previous contents are fully read
-      st_scatter<P::T, E, P::radix(S - 1), P::ns(S - 1)>(v, t, xb);
-      sync();
-#pragma unroll
-      for (int q = 0; q < E; ++q) v[q] = xb[spad(t + P::T * q)];
-      st_bfly<P::T, E, P::radix(S), P::ns(S), P::twoff(S), DIR, TWS>(v, t, tw);
-      Stages<N, E, DIR, S + 1, TWS>::run(v, t, xb, tw, sync);
-    }
-  }
-};
-
-template <int E>
-constexpr int pow2_max_threads() { return E <= 16 ? 512 : 256; }
 
 template <int N, int E, int DIR>
 __global__ void __launch_bounds__(pow2_max_threads<E>()) c2c_pow2_kernel(const Pow2Launch L) {

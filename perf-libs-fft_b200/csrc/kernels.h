@@ -184,6 +184,24 @@ cudaError_t launch_grouped(const GroupPhase& P, int grid, int smem_bytes, cudaSt
 int grouped_blocks_per_sm(int smem_bytes);
 int group_max_smem_elems();
 
+// Fused single-kernel real transforms for N = 2M, M a power of two
+// (real_fused.cu).  Distances count elements of each buffer's own type.
+enum FusedRealKind { FR_R2C = 0, FR_C2R = 1, FR_DCT2 = 2, FR_DST2 = 3 };
+struct RealFusedLaunch {
+  const void* in;
+  void* out;
+  int64_t howmany, idist, odist;
+  int g;  // transforms per CTA
+  float scale;
+  const float2* tw;    // stage twiddles of the length-M complex FFT
+  const float2* post;  // W_N^k, k = 0..M
+  const float2* rot;   // exp(-i pi k / 2N), k = 0..M
+  int pairs_in, pairs_out;  // real data may be moved as aligned float pairs
+};
+bool real_fused_supported(int m);
+int real_fused_e(int m);
+cudaError_t launch_real_fused(int kind, int m, const RealFusedLaunch& L, cudaStream_t st);
+
 // kernel entry points (c2c.cu)
 cudaError_t launch_c2c_reg(int e, int dir, const RegLaunch& L, cudaStream_t st);
 cudaError_t launch_c2c_tile(int maxe, int dir, const TileLaunch& L, cudaStream_t st);

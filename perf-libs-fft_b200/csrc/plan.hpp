@@ -134,6 +134,10 @@ int64_t next_smooth(int64_t n);
 std::unique_ptr<Node> make_realwrap_node(int kind, int64_t n, const Layout& lay, float scale, std::string* why,
                                          int wmode_in = 0, int wmode_out = 0);
 
+// One-kernel R2C / C2R / DCT-II / DST-II (FusedRealKind) for N = 2M, M a
+// power of two in [64, 8192], unit strides; nullptr when not applicable.
+std::unique_ptr<Node> make_real_fused_node(int kind, int64_t n, const Layout& lay, float scale);
+
 // Adjoint of a plan's transform (same scale, input/output layouts swapped):
 // the conjugate-direction C2C, or the transposed real transform expressed
 // as another kind with elementwise weights.

@@ -47,16 +47,20 @@ plfft_status_t build_plan(PlanData& p, std::string* why) {
         p.root = make_c2c_node(c.n, lay, c.payload, scale, c.precision, why);
         break;
       case TKind::R2C:
-        p.root = make_realwrap_node(RW_R2C, c.n, lay, scale, why);
+        p.root = make_real_fused_node(FR_R2C, c.n, lay, scale);
+        if (!p.root) p.root = make_realwrap_node(RW_R2C, c.n, lay, scale, why);
         break;
       case TKind::C2R:
-        p.root = make_realwrap_node(RW_C2R, c.n, lay, scale, why);
+        p.root = make_real_fused_node(FR_C2R, c.n, lay, scale);
+        if (!p.root) p.root = make_realwrap_node(RW_C2R, c.n, lay, scale, why);
         break;
       case TKind::R2R: {
         // plfft_r2r_kind_t -> RealWrapKind
         static const int map[] = {RW_DCT1, RW_DCT2, RW_DCT3, RW_DCT4, RW_DST1, RW_DST2,
                                   RW_DST3, RW_DST4, RW_DHT,  RW_R2HC, RW_HC2R};
-        p.root = make_realwrap_node(map[c.payload], c.n, lay, scale, why);
+        if (c.payload == PLFFT_R2R_DCT_2) p.root = make_real_fused_node(FR_DCT2, c.n, lay, scale);
+        if (c.payload == PLFFT_R2R_DST_2) p.root = make_real_fused_node(FR_DST2, c.n, lay, scale);
+        if (!p.root) p.root = make_realwrap_node(map[c.payload], c.n, lay, scale, why);
         break;
       }
     }

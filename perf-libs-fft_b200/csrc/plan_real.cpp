@@ -1,5 +1,7 @@
 // Plan nodes for R2C, C2R and R2R built on a C2C plan (realwrap.cu).
 #include <algorithm>
+#include <cstdint>
+#include <cstdlib>
 #include <sstream>
 
 #include "plan.hpp"
@@ -103,6 +105,81 @@ std::unique_ptr<Node> make_realwrap_node(int kind, int64_t n, const Layout& lay,
   Layout inner{node->chunk, 1, node->len, 1, node->len};
   node->inner = make_c2c_node(node->len, inner, wrap_dir(kind), 1.0f, 0, why);
   if (!node->inner) return nullptr;
+  return node;
+}
+
+}  // namespace plfft_b200
+
+namespace plfft_b200 {
+
+namespace {
+
+// One-kernel R2C / C2R / DCT-II / DST-II for N = 2M, M a power of two
+// (real_fused.cu); unit element stride.
+struct RealFusedNode : Node {
+  int kind = 0, m = 0;
+  RealFusedLaunch base{};
+  DevBuf tab;
+  cudaError_t run(const void* in, void* out, void*, cudaStream_t st) const override {
+    RealFusedLaunch L = base;
+    L.in = in;
+    L.out = out;
+    const bool in_real = kind != FR_C2R, out_real = kind != FR_R2C;
+    L.pairs_in = in_real && (reinterpret_cast<uintptr_t>(in) % 8 == 0) && (L.howmany == 1 || L.idist % 2 == 0);
+    L.pairs_out = out_real && (reinterpret_cast<uintptr_t>(out) % 8 == 0) && (L.howmany == 1 || L.odist % 2 == 0);
+    return launch_real_fused(kind, m, L, st);
+  }
+  std::string describe() const override {
+    static const char* names[] = {"r2c", "c2r", "dct2", "dst2"};
+    std::ostringstream o;
+    o << "(" << names[kind] << "-fused n=" << 2 * m << " m=" << m << " e=" << real_fused_e(m) << " g=" << base.g
+      << ")";
+    return o.str();
+  }
+};
+
+}  // namespace
+
+std::unique_ptr<Node> make_real_fused_node(int kind, int64_t n, const Layout& lay, float scale) {
+  if (n % 2 || !real_fused_supported(int(n / 2)) || lay.istride != 1 || lay.ostride != 1) return nullptr;
+  if (std::getenv("PLFFT_B200_NO_FUSED_REAL")) return nullptr;
+  const int m = int(n / 2);
+  const int e = real_fused_e(m);
+  std::vector<int> radices;
+  int rest = m, ke = 0;
+  while (rest % e == 0 && rest > 1) {
+    rest /= e;
+    ++ke;
+  }
+  if (rest > 1) radices.push_back(rest);
+  for (int i = 0; i < ke; ++i) radices.push_back(e);
+  std::vector<float2> tw;
+  make_desc(m, radices, tw);
+  const size_t post_off = tw.size();
+  for (int k = 0; k <= m; ++k) {  // W_N^k
+    double c, s;
+    unit_root(k, n, c, s);
+    tw.push_back(make_float2(float(c), float(-s)));
+  }
+  const size_t rot_off = tw.size();
+  for (int k = 0; k <= m; ++k) {  // exp(-i pi k / 2N) = W_{4N}^k
+    double c, s;
+    unit_root(k, 4 * n, c, s);
+    tw.push_back(make_float2(float(c), float(-s)));
+  }
+  auto node = std::make_unique<RealFusedNode>();
+  node->kind = kind;
+  node->m = m;
+  if (node->tab.upload(tw) != cudaSuccess) return nullptr;
+  const int t = m / e;
+  node->base.howmany = lay.howmany;
+  node->base.idist = lay.idist;
+  node->base.odist = lay.odist;
+  node->base.g = std::max(1, 128 / t);
+  node->base.scale = scale;
+  node->base.tw = node->tab.as<float2>();
+  node->base.post = node->tab.as<float2>() + post_off;
+  node->base.rot = node->tab.as<float2>() + rot_off;
   return node;
 }
 

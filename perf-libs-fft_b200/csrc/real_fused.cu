@@ -1,0 +1,213 @@
+// Fused real-data transforms for N = 2M with M a power of two: one kernel,
+// one pass over HBM.
+//
+// R2C  : the N reals are read as M complex values z_m = x_{2m} + i x_{2m+1};
+//        Z = DFT_M(z) runs in registers; then for k = 0..M
+//          X_k = E_k - i W_N^k O'_k,  E_k = (Z_k + conj Z_{M-k}) / 2,
+//                                     O'_k = (Z_k - conj Z_{M-k}) / 2.
+// C2R  : Z'_k = (X_k + conj X_{M-k}) + i conj(W_N^k) (X_k - conj X_{M-k})
+//        (imaginary parts of X_0 and X_M ignored), z = IDFT_M(Z') gives
+//        x_{2m} = Re z_m, x_{2m+1} = Im z_m.
+// DCT-II: Makhoul's permutation v_j = x_{2j} (j < M), v_{N-1-j} = x_{2j+1},
+//        V = DFT_N(v) by the R2C route above, then
+//        y_k = 2 Re(e^{-i pi k/2N} V_k), y_{N-k} = -2 Im(e^{-i pi k/2N} V_k).
+// DST-II: DST-II(x)_k = DCT-II((-1)^j x_j)_{N-1-k}.
+// These are the reference's R2C / C2R twiddle levels
+// (src/level_ab_t_r2c.cpp:17-120, src/level_ab_t_c2r.cpp:17-99) and its
+// DCT-II / DST-II pre/post passes (src/r2r_buffer_helper.hpp:316-335,
+// :455-469, :686-701, :828-854) folded into the on-chip FFT.
+#include "kernels.h"
+#include "pow2_stages.cuh"
+
+namespace plfft_b200 {
+
+// V_k (k = 0..M) of the real length-2M input from Z = DFT_M(z) held in
+// natural order in shared memory
+__device__ __forceinline__ float2 real_split(const float2* Z, int k, int m, const float2* post) {
+  const float2 zk = Z[k == m ? 0 : k];
+  const float2 zm = Z[k == 0 ? 0 : m - k];
+  const float2 cm = make_float2(zm.x, -zm.y);
+  const float2 e = cscale(cadd(zk, cm), 0.5f);
+  const float2 o = cscale(csub(zk, cm), 0.5f);
+  const float2 wo = cmul(__ldg(post + k), o);
+  return make_float2(e.x + wo.y, e.y - wo.x);  // e - i * wo
+}
+
+template <int M, int E, int KIND, class Sync>
+__device__ __forceinline__ void finish_real(float2 (&v)[E], const RealFusedLaunch& L, float2* mine, int t,
+                                            int64_t b, bool live, Sync sync) {
+  using P = P2<M, E>;
+  constexpr int T = P::T;
+  constexpr int N = 2 * M;
+  const float s = L.scale;
+  if constexpr (KIND == FR_C2R) {
+    if (!live) return;
+    float* x = static_cast<float*>(L.out) + b * L.odist;
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+      const int m = t + T * q;
+      const float2 z = cscale(v[q], s);
+      if (L.pairs_out) {
+        reinterpret_cast<float2*>(x)[m] = z;
+      } else {
+        x[2 * m] = z.x;
+        x[2 * m + 1] = z.y;
+      }
+    }
+  } else {
+    sync();  // last exchange fully read
+#pragma unroll
+    for (int q = 0; q < E; ++q) mine[t + T * q] = v[q];
+    sync();
+    if (!live) return;
+    // k = t + T*j for j < E covers 0..M-1; thread 0 also takes k = M
+    for (int j = 0; j <= E; ++j) {
+      const int k = j < E ? t + T * j : M;
+      if (j == E && t != 0) break;
+      const float2 V = real_split(mine, k, M, L.post);
+      if constexpr (KIND == FR_R2C) {
+        static_cast<float2*>(L.out)[b * L.odist + k] = cscale(V, s);
+      } else {
+        const float2 c = cmul(__ldg(L.rot + k), V);
+        float* y = static_cast<float*>(L.out) + b * L.odist;
+        const float yk = 2.f * c.x * s, ynk = -2.f * c.y * s;
+        if constexpr (KIND == FR_DCT2) {
+          y[k] = yk;
+          if (k > 0 && k < M) y[N - k] = ynk;
+        } else {
+          y[N - 1 - k] = yk;
+          if (k > 0 && k < M) y[k - 1] = ynk;
+        }
+      }
+    }
+  }
+}
+
+template <int M, int E, int KIND>
+__global__ void __launch_bounds__(pow2_max_threads<E>()) real_fused_kernel(const RealFusedLaunch L) {
+  using P = P2<M, E>;
+  constexpr int T = P::T;
+  constexpr int N = 2 * M;
+  constexpr int PITCH = (spad_len_c(M) + 1) & ~1;
+  constexpr int DIR = KIND == FR_C2R ? 1 : -1;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  const int G = L.g;
+  const int grp = threadIdx.x / T;
+  const int t = threadIdx.x - grp * T;
+  const int64_t b = int64_t(blockIdx.x) * G + grp;
+  const bool live = b < L.howmany;
+  float2* mine = reinterpret_cast<float2*>(smraw) + grp * PITCH;
+  auto sync = [&]() {
+    if constexpr (T <= 32)
+      __syncwarp();
+    else
+      __syncthreads();
+  };
+
+  float2 v[E];
+  if constexpr (KIND == FR_R2C) {
+    const float* x = static_cast<const float*>(L.in) + (live ? b * L.idist : 0);
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+      const int m = t + T * q;
+      if (!live)
+        v[q] = make_float2(0.f, 0.f);
+      else if (L.pairs_in)
+        v[q] = reinterpret_cast<const float2*>(x)[m];
+      else
+        v[q] = make_float2(x[2 * m], x[2 * m + 1]);
+    }
+  } else if constexpr (KIND == FR_C2R) {
+    const float2* X = static_cast<const float2*>(L.in) + (live ? b * L.idist : 0);
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+      const int k = t + T * q;
+      if (!live) {
+        v[q] = make_float2(0.f, 0.f);
+        continue;
+      }
+      float2 xk = X[k], xm = X[M - k];
+      if (k == 0) {
+        xk.y = 0.f;
+        xm.y = 0.f;
+      }
+      const float2 cm = make_float2(xm.x, -xm.y);
+      const float2 a = cadd(xk, cm);
+      const float2 d = csub(xk, cm);
+      const float2 wd = cmulc(d, __ldg(L.post + k));  // conj(W_N^k) * d
+      v[q] = cadd(a, make_float2(-wd.y, wd.x));       // a + i * wd
+    }
+  } else {
+    // DCT-II / DST-II: stage the N reals in the slot, then gather the
+    // Makhoul-permuted pairs
+    float* xs = reinterpret_cast<float*>(mine);
+    const float* x = static_cast<const float*>(L.in) + (live ? b * L.idist : 0);
+    for (int f = t; f < N; f += T) {
+      float val = live ? x[f] : 0.f;
+      if constexpr (KIND == FR_DST2) val = (f & 1) ? -val : val;
+      xs[f] = val;
+    }
+    sync();
+    auto perm = [&](int j) { return j < M ? xs[2 * j] : xs[2 * (N - 1 - j) + 1]; };
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+      const int m = t + T * q;
+      v[q] = make_float2(perm(2 * m), perm(2 * m + 1));
+    }
+  }
+
+  st_bfly<T, E, P::radix(0), 1, 0, DIR>(v, t, L.tw);
+  Stages<N / 2, E, DIR, 1>::run(v, t, mine, L.tw, sync);
+  finish_real<M, E, KIND>(v, L, mine, t, b, live, sync);
+}
+
+int real_fused_e(int m) {
+  if (m <= 512) return 16;
+  if (m <= 2048) return 32;
+  if (m == 4096) return 16;
+  return 32;
+}
+
+bool real_fused_supported(int m) { return m >= 64 && m <= 8192 && (m & (m - 1)) == 0; }
+
+template <int M, int E, int KIND>
+static cudaError_t run_real_fused(const RealFusedLaunch& L, cudaStream_t st) {
+  constexpr int T = M / E;
+  constexpr int PITCH = (spad_len_c(M) + 1) & ~1;
+  const int smem = L.g * PITCH * int(sizeof(float2));
+  if (smem > 32 * 1024) {  // leave room for static shared memory
+    const cudaError_t e =
+        cudaFuncSetAttribute(real_fused_kernel<M, E, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+  }
+  const int64_t blocks = (L.howmany + L.g - 1) / L.g;
+  real_fused_kernel<M, E, KIND><<<dim3(unsigned(blocks)), dim3(T * L.g), smem, st>>>(L);
+  return cudaGetLastError();
+}
+
+template <int M, int E>
+static cudaError_t run_real_fused_kind(int kind, const RealFusedLaunch& L, cudaStream_t st) {
+  switch (kind) {
+    case FR_R2C: return run_real_fused<M, E, FR_R2C>(L, st);
+    case FR_C2R: return run_real_fused<M, E, FR_C2R>(L, st);
+    case FR_DCT2: return run_real_fused<M, E, FR_DCT2>(L, st);
+    case FR_DST2: return run_real_fused<M, E, FR_DST2>(L, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_real_fused(int kind, int m, const RealFusedLaunch& L, cudaStream_t st) {
+  switch (m) {
+    case 64: return run_real_fused_kind<64, 16>(kind, L, st);
+    case 128: return run_real_fused_kind<128, 16>(kind, L, st);
+    case 256: return run_real_fused_kind<256, 16>(kind, L, st);
+    case 512: return run_real_fused_kind<512, 16>(kind, L, st);
+    case 1024: return run_real_fused_kind<1024, 32>(kind, L, st);
+    case 2048: return run_real_fused_kind<2048, 32>(kind, L, st);
+    case 4096: return run_real_fused_kind<4096, 16>(kind, L, st);
+    case 8192: return run_real_fused_kind<8192, 32>(kind, L, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace plfft_b200

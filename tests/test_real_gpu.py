@@ -139,3 +139,65 @@ def test_r2r_strided(kind):
     y = run_plan(plan, x, span(hm, od, n, os_), torch.float32)
     ref = oracle.r2r(gather(x, hm, id_, n, is_).astype(np.float64), kind)
     assert oracle.rel_l2(gather(y, hm, od, n, os_), ref) <= oracle.fp32_tol(2 * n)
+
+
+FUSED_N = [128, 256, 512, 1024, 2048, 4096, 8192, 16384]
+
+
+@pytest.mark.parametrize("n", FUSED_N)
+@pytest.mark.parametrize("pad", [0, 1])
+def test_fused_r2c_c2r(n, pad):
+    """One-kernel R2C/C2R (N = 2M, M a power of two); pad=1 makes the real
+    distance odd so real pairs are not 8-byte aligned (scalar path)."""
+    import torch
+
+    hm = 5
+    h = n // 2 + 1
+    rid, cid = n + pad, h + pad
+    rng = np.random.default_rng(n + pad)
+    x = rng.uniform(-1, 1, span(hm, rid, n, 1)).astype(np.float32)
+    f = plfft.make_plan("r2c", n, hm, 1, rid, 1, cid)
+    assert "fused" in f.describe(), f.describe()
+    y = run_plan(f, x, span(hm, cid, h, 1), torch.complex64)
+    ref = oracle.r2c(gather(x, hm, rid, n, 1).astype(np.float64))
+    assert oracle.rel_l2(gather(y, hm, cid, h, 1), ref) <= oracle.fp32_tol(n)
+    X = (rng.uniform(-1, 1, (hm, h)) + 1j * rng.uniform(-1, 1, (hm, h))).astype(np.complex64)
+    b = plfft.make_plan("c2r", n, hm, 1, h, 1, rid)
+    assert "fused" in b.describe(), b.describe()
+    z = run_plan(b, X.ravel(), span(hm, rid, n, 1), torch.float32)
+    refz = oracle.c2r(X.astype(np.complex128), n)
+    assert oracle.rel_l2(gather(z, hm, rid, n, 1), refz) <= oracle.fp32_tol(n)
+
+
+@pytest.mark.parametrize("kind", ["DCT_2", "DST_2"])
+@pytest.mark.parametrize("n", [128, 1024, 2048, 4096, 16384])
+def test_fused_dct2_dst2(kind, n):
+    import torch
+
+    hm = 3
+    rng = np.random.default_rng(n)
+    x = rng.uniform(-1, 1, hm * n).astype(np.float32)
+    plan = plfft.make_plan("r2r", n, hm, r2r_kind=plfft.R2RKind[kind])
+    assert "fused" in plan.describe(), plan.describe()
+    y = run_plan(plan, x, hm * n, torch.float32).reshape(hm, n)
+    ref = oracle.r2r(x.reshape(hm, n).astype(np.float64), kind)
+    assert oracle.rel_l2(y, ref) <= oracle.fp32_tol(2 * n)
+
+
+@pytest.mark.parametrize("n", [1024, 4096])
+def test_fused_r2c_in_place(n):
+    """In-place R2C with the padded layout (each member's output over its own input)."""
+    import torch
+
+    hm = 4
+    h = n // 2 + 1
+    rng = np.random.default_rng(3)
+    buf = np.zeros(hm * 2 * h, np.float32)
+    xs = rng.uniform(-1, 1, (hm, n)).astype(np.float32)
+    for b in range(hm):
+        buf[b * 2 * h: b * 2 * h + n] = xs[b]
+    d = torch.from_numpy(buf).cuda()
+    plan = plfft.make_plan("r2c", n, hm, 1, 2 * h, 1, h, alias=plfft.IoAlias.MAY_ALIAS)
+    plan.execute(d.data_ptr(), d.data_ptr())
+    y = d.cpu().numpy().view(np.complex64).reshape(hm, h)
+    assert oracle.rel_l2(y, oracle.r2c(xs.astype(np.float64))) <= oracle.fp32_tol(n)
