@@ -14,6 +14,7 @@
 //                  src/level_ab_t_c2c.cpp:49-80).
 #include "kernels.h"
 #include "stockham.cuh"
+#include "ptx.cuh"
 
 namespace plfft_b200 {
 
@@ -90,14 +91,15 @@ __global__ void __launch_bounds__(PLFFT_B200_TILE_THREADS(MAXE), 1) c2c_tile_ker
   if (iks == 1) {
     for (int f = tid; f < total; f += nthr) {
       const int c = f / n, k = f - c * n;
-      smem[c * ld + spad(k)] = L.in[ibase[c] + k];
+      cp_async8(smem + c * ld + spad(k), L.in + ibase[c] + k);
     }
   } else {
     for (int f = tid; f < total; f += nthr) {
       const int k = f / cnt, c = f - k * cnt;
-      smem[c * ld + spad(k)] = L.in[ibase[c] + k * iks];
+      cp_async8(smem + c * ld + spad(k), L.in + ibase[c] + k * iks);
     }
   }
+  cp_async_wait_all();
   __syncthreads();
   smem_fft<MAXE, DIR>(smem, cnt, ld, L.desc, L.tw, tid, nthr);
 

@@ -202,6 +202,25 @@ bool real_fused_supported(int m);
 int real_fused_e(int m);
 cudaError_t launch_real_fused(int kind, int m, const RealFusedLaunch& L, cudaStream_t st);
 
+// One pass of a power-of-two four-step transform (fourstep.cu): `count`
+// sub-transforms of length nl, sub-transform g = (member g / ncols, column
+// g % ncols), element k at base + member*mdist + column*cd + k*ks.
+struct FourStepLaunch {
+  const float2* in;
+  float2* out;
+  int64_t count, ncols;
+  int64_t imdist, icd, iks;
+  int64_t omdist, ocd, oks;
+  int c;  // sub-transforms per CTA
+  float scale;
+  const float2* tw;  // stage twiddles of length nl
+  TwoLevel post;     // W_n^{column * k} on the outputs when post.n != 0
+};
+bool fourstep_pass_supported(int nl);
+int fourstep_pass_e(int nl);
+int fourstep_pass_smem(int nl, int c);
+cudaError_t launch_fourstep_pass(int nl, int dir, const FourStepLaunch& L, cudaStream_t st);
+
 // kernel entry points (c2c.cu)
 cudaError_t launch_c2c_reg(int e, int dir, const RegLaunch& L, cudaStream_t st);
 cudaError_t launch_c2c_tile(int maxe, int dir, const TileLaunch& L, cudaStream_t st);

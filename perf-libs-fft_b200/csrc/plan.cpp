@@ -384,6 +384,97 @@ int64_t four_step_split(int64_t n) {
   return best;
 }
 
+// power-of-two four-step: both passes are static register kernels
+// (fourstep.cu); members are processed in chunks whose intermediate stays
+// near L2 size
+struct C2CFourStepPow2Node : Node {
+  int64_t n = 0, n1 = 0, n2 = 0, chunk = 1;
+  int dir = -1;
+  Layout lay{};
+  FourStepLaunch p1{}, p2{};
+  DevBuf tw1, tw2, lo, hi;
+  size_t workspace() const override { return size_t(chunk) * size_t(n) * sizeof(float2); }
+  int launches() const override { return int(2 * ((lay.howmany + chunk - 1) / chunk)); }
+  cudaError_t run(const void* in, void* out, void* ws, cudaStream_t st) const override {
+    const float2* x = static_cast<const float2*>(in);
+    float2* y = static_cast<float2*>(out);
+    float2* s = static_cast<float2*>(ws);
+    for (int64_t m0 = 0; m0 < lay.howmany; m0 += chunk) {
+      const int64_t cnt = std::min(chunk, lay.howmany - m0);
+      FourStepLaunch a = p1;
+      a.in = x + m0 * lay.idist;
+      a.out = s;
+      a.count = cnt * n2;
+      cudaError_t e = launch_fourstep_pass(int(n1), dir, a, st);
+      if (e != cudaSuccess) return e;
+      FourStepLaunch b = p2;
+      b.in = s;
+      b.out = y + m0 * lay.odist;
+      b.count = cnt * n1;
+      e = launch_fourstep_pass(int(n2), dir, b, st);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+  std::string describe() const override {
+    std::ostringstream o;
+    o << "(c2c-four-step-pow2 n=" << n << " " << n1 << "x" << n2 << " chunk=" << chunk << " c=" << p1.c << "/"
+      << p2.c << ")";
+    return o.str();
+  }
+};
+
+static int fourstep_c(int nl) {
+  const int t = nl / fourstep_pass_e(nl);
+  int c = std::min(env_int("PLFFT_B200_FS_C", 8), std::max(1, 512 / t));
+  while (c > 1 && fourstep_pass_smem(nl, c) > 200 * 1024) c /= 2;
+  return c;
+}
+
+static std::unique_ptr<Node> make_four_step_pow2(int64_t n, const Layout& lay, int dir, float scale) {
+  if (!is_pow2(n) || std::getenv("PLFFT_B200_NO_FS_POW2")) return nullptr;
+  int b = ilog2(n);
+  const int64_t n1 = int64_t(1) << (b / 2), n2 = n / n1;
+  if (!fourstep_pass_supported(int(n1)) || !fourstep_pass_supported(int(n2))) return nullptr;
+  auto node = std::make_unique<C2CFourStepPow2Node>();
+  node->n = n;
+  node->n1 = n1;
+  node->n2 = n2;
+  node->dir = dir;
+  node->lay = lay;
+  const int64_t target = int64_t(env_int("PLFFT_B200_FS_CHUNK_MB", 256)) << 20;
+  node->chunk = std::max<int64_t>(1, std::min<int64_t>(lay.howmany, target / (n * 8)));
+  auto stage_table = [&](int64_t nl, DevBuf& buf) {
+    const int e = fourstep_pass_e(int(nl));
+    std::vector<int> radices;
+    int64_t rest = nl;
+    int ke = 0;
+    while (rest % e == 0 && rest > 1) {
+      rest /= e;
+      ++ke;
+    }
+    if (rest > 1) radices.push_back(int(rest));
+    for (int i = 0; i < ke; ++i) radices.push_back(e);
+    std::vector<float2> tw;
+    make_desc(int(nl), radices, tw);
+    return buf.upload(tw) == cudaSuccess;
+  };
+  if (!stage_table(n1, node->tw1) || !stage_table(n2, node->tw2)) return nullptr;
+  const int64_t L = int64_t(1) << ((ilog2(n) + 1) / 2);
+  std::vector<float2> lo(L), hi((n + L - 1) / L);
+  for (int64_t i = 0; i < L; ++i) lo[i] = root_f(i, n, -1);
+  for (size_t i = 0; i < hi.size(); ++i) hi[i] = root_f(int64_t(i) * L, n, -1);
+  if (node->lo.upload(lo) != cudaSuccess || node->hi.upload(hi) != cudaSuccess) return nullptr;
+  // pass 1: sub-transform g = (member, column n2 index), element k = n1 index
+  node->p1 = FourStepLaunch{nullptr, nullptr, 0, n2, lay.idist, lay.istride, n2 * lay.istride, n, 1, n2,
+                            fourstep_c(int(n1)), 1.0f, node->tw1.as<float2>(),
+                            TwoLevel{node->lo.as<float2>(), node->hi.as<float2>(), n, int(L)}};
+  // pass 2: sub-transform g = (member, row k1), element k = n2 index
+  node->p2 = FourStepLaunch{nullptr, nullptr, 0, n1, n, n2, 1, lay.odist, lay.ostride, n1 * lay.ostride,
+                            fourstep_c(int(n2)), scale, node->tw2.as<float2>(), TwoLevel{nullptr, nullptr, 0, 1}};
+  return node;
+}
+
 static std::unique_ptr<Node> make_four_step(int64_t n, const Layout& lay, int dir, float scale,
                                             std::string* why) {
   const int64_t best = four_step_split(n);
@@ -460,6 +551,7 @@ std::unique_ptr<Node> make_c2c_node(int64_t n, const Layout& lay, int dir, float
     auto t = make_tile(n, lay.howmany, ia, oa, dir, scale, interleaved, why);
     if (t) return t;
   }
+  if (auto fs = make_four_step_pow2(n, lay, dir, scale)) return fs;
   if (is_smooth(n)) return make_four_step(n, lay, dir, scale, why);
   return make_conv_node(n, lay, dir, scale, why);
 }
