@@ -361,6 +361,70 @@ class AdjointWorkload(PlanWorkload):
         self.launches *= 2
 
 
+class Q15Workload(PlanWorkload):
+    """Q0.15 fixed-point C2C (int16 re/im pairs, scaled by 1/N)."""
+
+    dtype = "int16"
+
+    def __init__(self, name, desc, n, batch):
+        super().__init__(name, desc, "c2c", n, batch)
+
+    def sizes(self):
+        return self.n * self.batch * 4, self.n * self.batch * 4
+
+    def config(self):
+        c = super().config()
+        c["precision"] = "q15 (bit-exact to the reference's fixed-point codelets)"
+        return c
+
+    def setup(self, gen):
+        import torch
+
+        import plfft
+
+        self.plan = plfft.make_plan("c2c", self.n, self.batch, data_type=plfft.DataType.Q15)
+        ib, ob = self.sizes()
+        self.sets = max(2, -(-4 * L2_BYTES // (ib + ob)))
+        # int16 re/im uniform in [-2^14, 2^14), two per 32-bit word
+        self.ins = [torch.randint(-(1 << 14), 1 << 14, (ib // 2,), dtype=torch.int16, device="cuda",
+                                  generator=gen).view(torch.int32) for _ in range(self.sets)]
+        self.outs = [torch.empty(ob // 4, dtype=torch.int32, device="cuda") for _ in range(self.sets)]
+        self.ws = torch.empty(1, dtype=torch.uint8, device="cuda")
+        self.launches = self.plan.launch_count()
+
+    def e2e(self, steps):
+        import torch
+
+        ib, ob = self.sizes()
+        hx = self.ins[0].cpu().pin_memory()
+        hy = torch.empty(ob // 4, dtype=torch.int32).pin_memory()
+        self.plan.execute(hx.data_ptr(), hy.data_ptr())
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(torch.cuda.default_stream())
+        for _ in range(steps):
+            self.plan.execute(hx.data_ptr(), hy.data_ptr())
+        e1.record(torch.cuda.default_stream())
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, ib, ob, "plfft_plan_execute(host pinned buffers)"
+
+    def cpu_sample(self, threads):
+        import numpy as np
+
+        import oracle
+
+        m = min(self.batch, 4096)
+        rng = np.random.default_rng(0)
+        x = rng.integers(-(1 << 14), 1 << 14, (m, self.n, 2)).astype(np.int16)
+        oracle.q15_c2c(x[:16], -1)
+        reps = 3
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            oracle.q15_c2c(x, -1)
+        dt = (time.perf_counter() - t0) / reps
+        return dt, self.algo_bytes() * m / self.batch, f"{m} of {self.batch} transforms, bit-exact Q0.15 C restatement (oracle/q15.c, 1 thread)"
+
+
 def make_workload(name):
     table = {
         "c2c_n1024_b4096": lambda: PlanWorkload("c2c_n1024_b4096", "plain C2C FP32 forward N=1024 batch=4096",
@@ -375,13 +439,14 @@ def make_workload(name):
         "c2c_n1m_b64": lambda: PlanWorkload("c2c_n1m_b64", "C2C FP32 N=2^20 batch=64", "c2c", 1 << 20, 64),
         "c2c_n64k_b1024": lambda: PlanWorkload("c2c_n64k_b1024", "C2C FP32 N=2^16 batch=1024", "c2c", 1 << 16, 1024),
         "grouped_4000": lambda: GroupedWorkload(),
+        "q15_n256_b16384": lambda: Q15Workload("q15_n256_b16384", "C2C Q0.15 forward N=256 batch=16384", 256, 16384),
         "diff_r2c_n8192_b1024": lambda: AdjointWorkload(),
     }
     return table[name]()
 
 
 WORKLOAD_NAMES = ["c2c_n1024_b4096", "r2c_c2r_n4096_b8192", "dct2_n1024_b4096", "dst2_n1024_b4096", "c2c_n1m_b64",
-                  "c2c_n64k_b1024", "grouped_4000", "diff_r2c_n8192_b1024"]
+                  "c2c_n64k_b1024", "grouped_4000", "diff_r2c_n8192_b1024", "q15_n256_b16384"]
 
 
 # --------------------------------------------------------------------------
@@ -494,7 +559,7 @@ def main():
         cpu = cpu_baseline(w)
         line = {"metric": f"{w.name} GB/s (algorithmic bytes)", "value": cpu["value"], "unit": "GB/s",
                 "impl": "reference", "n_gpus": args.gpus, "steps": 1, "warmup": 1,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64" if w.dtype == "f32" else w.dtype,
                 "data": "synthetic (seeded U[-1,1))", "config": w.config(), "cpu_baseline": cpu,
                 "e2e": {"value": cpu["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))

@@ -124,3 +124,43 @@ def rel_l2(got, ref):
 def fp32_tol(n):
     """FP32 gate: rel-L2 <= 4 * log2(N) * 2^-24."""
     return 4.0 * max(1.0, np.log2(max(n, 2))) * 2.0 ** -24
+
+
+# ---------------------------------------------------------------------------
+# Q0.15 fixed point (oracle/q15.c): bit-exact restatement, n power of two <= 256
+# ---------------------------------------------------------------------------
+_LIBQ = None
+
+
+def _libq():
+    global _LIBQ
+    if _LIBQ is None:
+        path = os.path.join(_HERE, "lib", "liboracle_q15.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"oracle library missing: {path} (run make -C oracle)")
+        L = ctypes.CDLL(path)
+        i64 = ctypes.c_int64
+        dp = ctypes.c_void_p
+        L.oracle_q15_c2c.argtypes = [dp, dp, i64, i64, i64, i64, ctypes.c_int]
+        L.oracle_q15_c2c.restype = ctypes.c_int
+        L.oracle_q15_twiddles.argtypes = [i64, ctypes.c_int, dp]
+        L.oracle_q15_twiddles.restype = None
+        _LIBQ = L
+    return _LIBQ
+
+
+def q15_c2c(x, direction=-1):
+    """x: int16 [howmany, n, 2] (re, im) -> int16 [howmany, n, 2], scaled by 1/n."""
+    x = np.ascontiguousarray(x, dtype=np.int16)
+    hm, n = x.shape[0], x.shape[1]
+    y = np.empty_like(x)
+    rc = _libq().oracle_q15_c2c(_ptr(x), _ptr(y), n, hm, n, n, int(direction))
+    if rc != 0:
+        raise ValueError(f"q15 oracle: unsupported length {n}")
+    return y
+
+
+def q15_twiddles(n, direction=-1):
+    w = np.empty(max(0, n // 16 - 1) * 15 * 4, np.int16)
+    _libq().oracle_q15_twiddles(n, int(direction), _ptr(w))
+    return w

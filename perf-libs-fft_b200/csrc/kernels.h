@@ -221,6 +221,18 @@ int fourstep_pass_e(int nl);
 int fourstep_pass_smem(int nl, int c);
 cudaError_t launch_fourstep_pass(int nl, int dir, const FourStepLaunch& L, cudaStream_t st);
 
+// Q0.15 fixed-point C2C (q15.cu): power-of-two n <= 256; elements are
+// int16 (re, im) pairs handled as one 32-bit word; strides in elements.
+struct Q15Launch {
+  const int* in;
+  int* out;
+  int64_t howmany;
+  int64_t istride, idist, ostride, odist;
+  const int2* tw;  // n >= 32: per row j >= 1 and input i >= 1, words (c, s) and (-s, c)
+};
+bool q15_supported(int64_t n);
+cudaError_t launch_q15(int n, int dir, const Q15Launch& L, cudaStream_t st);
+
 // kernel entry points (c2c.cu)
 cudaError_t launch_c2c_reg(int e, int dir, const RegLaunch& L, cudaStream_t st);
 cudaError_t launch_c2c_tile(int maxe, int dir, const TileLaunch& L, cudaStream_t st);

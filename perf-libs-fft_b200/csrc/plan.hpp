@@ -118,6 +118,9 @@ int64_t four_step_split(int64_t n);
 std::unique_ptr<Node> make_c2c_node(int64_t n, const Layout& lay, int dir, float scale,
                                     int precision, std::string* why);
 
+// Q0.15 fixed-point C2C node (plan_q15.cpp); nullptr (with why) if unsupported.
+std::unique_ptr<Node> make_q15_node(int64_t n, const Layout& lay, int dir, std::string* why);
+
 // FP64 host helpers for table generation (plan_conv.cpp)
 using cd = std::complex<double>;
 std::vector<cd> host_fft(const std::vector<cd>& x, int sign);

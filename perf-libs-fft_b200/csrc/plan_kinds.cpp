@@ -64,6 +64,12 @@ plfft_status_t build_plan(PlanData& p, std::string* why) {
         break;
       }
     }
+  } else if (c.data_type == PLFFT_DATA_TYPE_Q15 && c.kind == TKind::C2C) {
+    if (c.scale != 1.0) {
+      if (why) *why = "fixed-point transforms are scaled by 1/n and take no extra scale";
+    } else {
+      p.root = make_q15_node(c.n, lay, c.payload, why);
+    }
   } else if ((c.data_type == PLFFT_DATA_TYPE_Q15 || c.data_type == PLFFT_DATA_TYPE_Q7) &&
              c.kind == TKind::R2R) {
     // fixed-point real-to-real has no implementation (reference src/plfft.cpp:248-261)
