@@ -374,3 +374,20 @@ def make_plan(kind, n, howmany=1, istride=1, idist=None, ostride=1, odist=None, 
         return Plan(cfg)
     finally:
         cfg.destroy()
+
+
+# ---------------------------------------------------------------------------
+# multi-GPU: contiguous batch shards, no collective on the data path
+# ---------------------------------------------------------------------------
+def shard_range(howmany, world, rank):
+    """First member and member count of `rank`'s contiguous share of a batch.
+
+    Members of a batch are independent, so a batch spread over `world`
+    processes (one per GPU) needs no exchange: rank r transforms members
+    [first, first + count) with a plan of howmany = count whose input and
+    output pointers are offset by first * idist and first * odist.
+    """
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError(f"rank {rank} outside world {world}")
+    first = howmany * rank // world
+    return first, howmany * (rank + 1) // world - first

@@ -71,7 +71,7 @@ def test_q15_strided_layouts_and_guard_words(n):
 
     plan = plfft.make_plan("c2c", n, hm, hm, 1, os_, od, direction=-1, data_type=plfft.DataType.Q15)
     d_in = torch.from_numpy(inter.view(np.int32).ravel().copy()).cuda()
-    sentinel = np.int32(0x5A5AA5A5 - (1 << 32))
+    sentinel = np.int32(0x5A5AA5A5)
     d_out = torch.full((total,), int(sentinel), dtype=torch.int32, device="cuda")
     plan.execute(d_in.data_ptr(), d_out.data_ptr())
     got = d_out.cpu().numpy()
