@@ -438,6 +438,12 @@ def make_workload(name):
                                                  1024, 4096, r2r="DST_2"),
         "c2c_n1m_b64": lambda: PlanWorkload("c2c_n1m_b64", "C2C FP32 N=2^20 batch=64", "c2c", 1 << 20, 64),
         "c2c_n64k_b1024": lambda: PlanWorkload("c2c_n64k_b1024", "C2C FP32 N=2^16 batch=1024", "c2c", 1 << 16, 1024),
+        "c2c_n1m_b64_split_bf16": lambda: PlanWorkload("c2c_n1m_b64_split_bf16",
+                                                       "C2C N=2^20 batch=64, split-BF16 tensor-core stages",
+                                                       "c2c", 1 << 20, 64, precision=1),
+        "c2c_n64k_b1024_split_bf16": lambda: PlanWorkload("c2c_n64k_b1024_split_bf16",
+                                                          "C2C N=2^16 batch=1024, split-BF16 tensor-core stages",
+                                                          "c2c", 1 << 16, 1024, precision=1),
         "grouped_4000": lambda: GroupedWorkload(),
         "q15_n256_b16384": lambda: Q15Workload("q15_n256_b16384", "C2C Q0.15 forward N=256 batch=16384", 256, 16384),
         "diff_r2c_n8192_b1024": lambda: AdjointWorkload(),
@@ -446,7 +452,8 @@ def make_workload(name):
 
 
 WORKLOAD_NAMES = ["c2c_n1024_b4096", "r2c_c2r_n4096_b8192", "dct2_n1024_b4096", "dst2_n1024_b4096", "c2c_n1m_b64",
-                  "c2c_n64k_b1024", "grouped_4000", "diff_r2c_n8192_b1024", "q15_n256_b16384"]
+                  "c2c_n64k_b1024", "c2c_n1m_b64_split_bf16", "c2c_n64k_b1024_split_bf16", "grouped_4000",
+                  "diff_r2c_n8192_b1024", "q15_n256_b16384"]
 
 
 # --------------------------------------------------------------------------
@@ -537,7 +544,8 @@ def cpu_baseline(w):
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: enough for about 1 s of timed work, at least 200)")
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2c_n1024_b4096", choices=WORKLOAD_NAMES)
@@ -588,19 +596,34 @@ def main():
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
 
-    sampler = ClockSampler(local)
-    sampler.start()
     for i in range(args.warmup):
         w.step(i, sh)
     torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if args.steps is None:
+        # size the timed region to about one second (clock samples need it)
+        ev0.record(stream)
+        for i in range(20):
+            w.step(i, sh)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        est = ev0.elapsed_time(ev1) / 20
+        steps = [max(200, min(200000, int(1000.0 / max(est, 1e-4))))]
+        if dist is not None:  # every rank times the same number of steps
+            t = torch.tensor(steps, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            steps = [int(t.item())]
+        args.steps = steps[0]
     barrier()
     torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(local)
+    sampler.start()
     ev0.record(stream)
     for i in range(args.steps):
         w.step(i, sh)
     ev1.record(stream)
     torch.cuda.synchronize()
+    clocks = sampler.stop()
     barrier()
     ms = ev0.elapsed_time(ev1)
     # per-step device time (each step bracketed by events)
@@ -617,7 +640,6 @@ def main():
         e2e_ms, hb, db, api = w.e2e(max(3, min(args.steps, 20)))
         e2e = {"value": w.algo_bytes() * world / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s",
                "h2d_bytes_per_step": hb, "d2h_bytes_per_step": db, "ms_per_step": e2e_ms, "api": api}
-    clocks = sampler.stop()
 
     if dist is not None:
         t = torch.tensor([ms, step_ms, e2e["ms_per_step"] if e2e else 0.0], device="cuda")
@@ -631,7 +653,10 @@ def main():
     abytes = w.algo_bytes()
     value = abytes * world / (ms_per_step * 1e-3) / 1e9
     peak, peak_kind = peaks()
-    achieved = abytes / (step_ms * 1e-3) / 1e9
+    # one launch per step: its average duration over the timed region;
+    # several: the median event-bracketed step (all of the step's kernels)
+    kernel_ms = ms_per_step if w.launches == 1 else step_ms
+    achieved = abytes / (kernel_ms * 1e-3) / 1e9
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(w)
@@ -646,7 +671,7 @@ def main():
             "gflops": w.flops() * world / (ms_per_step * 1e-3) / 1e9,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
-                         "traffic": profile_traffic(w.profile), "kernel_ms": step_ms,
+                         "traffic": profile_traffic(w.profile), "kernel_ms": kernel_ms,
                          "algorithmic_bytes_per_step": abytes, "launches_per_step": w.launches},
             "e2e": e2e,
             "gpu_launches": w.launches * args.steps,

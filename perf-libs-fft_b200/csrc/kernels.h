@@ -233,6 +233,14 @@ struct Q15Launch {
 bool q15_supported(int64_t n);
 cudaError_t launch_q15(int n, int dir, const Q15Launch& L, cudaStream_t st);
 
+// Split-BF16 tensor-core pass (split_bf16.cu): same addressing as a
+// four-step pass, on-chip length nl in {256, 4096} as radix-16 DFT-matrix
+// products; dftm = three 32x32 bf16 splits of the real DFT-16 matrix.
+bool split_bf16_pass_supported(int nl);
+int split_bf16_pass_c(int nl);
+cudaError_t launch_split_bf16_pass(int nl, int dir, const FourStepLaunch& L, const uint32_t* dftm,
+                                   cudaStream_t st);
+
 // kernel entry points (c2c.cu)
 cudaError_t launch_c2c_reg(int e, int dir, const RegLaunch& L, cudaStream_t st);
 cudaError_t launch_c2c_tile(int maxe, int dir, const TileLaunch& L, cudaStream_t st);

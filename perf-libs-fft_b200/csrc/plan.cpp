@@ -1,6 +1,8 @@
 // Planner: radix factorization, device twiddle tables and C2C schedules.
 #include "plan.hpp"
 
+#include <cstring>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -514,9 +516,146 @@ static std::unique_ptr<Node> make_four_step(int64_t n, const Layout& lay, int di
   return node;
 }
 
+// ---------------------------------------------------------------------------
+// split-BF16 tensor-core precision (split_bf16.cu): n = 256 or 4096 in one
+// pass, n = 256 x 256 and 256 x 4096 as a four-step pair of passes
+// ---------------------------------------------------------------------------
+static uint16_t bf16_rn(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  u += 0x7fffu + ((u >> 16) & 1u);  // round to nearest even (finite inputs)
+  return uint16_t(u >> 16);
+}
+static double bf16_val(uint16_t h) {
+  const uint32_t u = uint32_t(h) << 16;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return double(f);
+}
+
+// three bf16 splits of the real 32x32 form of the DFT-16 matrix
+// exp(dir 2 pi i iq / 16), packed two columns per 32-bit word
+static std::vector<uint32_t> split_dft16(int dir) {
+  std::vector<uint32_t> out(3 * 32 * 16);
+  for (int row = 0; row < 32; ++row)
+    for (int col = 0; col < 32; ++col) {
+      const int i = row & 15, q = col & 15;
+      const double ang = double(dir) * 2.0 * M_PI * double((i * q) % 16) / 16.0;
+      const double wr = std::cos(ang), wi = std::sin(ang);
+      // [Re W, -Im W; Im W, Re W]
+      const double a = row < 16 ? (col < 16 ? wr : -wi) : (col < 16 ? wi : wr);
+      double r = a;
+      for (int s = 0; s < 3; ++s) {
+        const uint16_t h = bf16_rn(float(r));
+        r -= bf16_val(h);
+        uint32_t& w = out[size_t(s) * 512 + size_t(row) * 16 + size_t(col / 2)];
+        w |= (col & 1) ? uint32_t(h) << 16 : uint32_t(h);
+      }
+    }
+  return out;
+}
+
+struct SplitBf16Node : Node {
+  int64_t n = 0, n1 = 0, n2 = 0, chunk = 1;  // n2 == 0: one pass of length n1
+  int dir = -1;
+  Layout lay{};
+  FourStepLaunch p1{}, p2{};
+  DevBuf tw1, tw2, lo, hi, dftm;
+  size_t workspace() const override { return n2 ? size_t(chunk) * size_t(n) * sizeof(float2) : 0; }
+  int launches() const override { return n2 ? int(2 * ((lay.howmany + chunk - 1) / chunk)) : 1; }
+  cudaError_t run(const void* in, void* out, void* ws, cudaStream_t st) const override {
+    const float2* x = static_cast<const float2*>(in);
+    float2* y = static_cast<float2*>(out);
+    const uint32_t* m = dftm.as<uint32_t>();
+    if (!n2) {
+      FourStepLaunch a = p1;
+      a.in = x;
+      a.out = y;
+      return launch_split_bf16_pass(int(n1), dir, a, m, st);
+    }
+    float2* s = static_cast<float2*>(ws);
+    for (int64_t m0 = 0; m0 < lay.howmany; m0 += chunk) {
+      const int64_t cnt = std::min(chunk, lay.howmany - m0);
+      FourStepLaunch a = p1;
+      a.in = x + m0 * lay.idist;
+      a.out = s;
+      a.count = cnt * n2;
+      cudaError_t e = launch_split_bf16_pass(int(n1), dir, a, m, st);
+      if (e != cudaSuccess) return e;
+      FourStepLaunch b = p2;
+      b.in = s;
+      b.out = y + m0 * lay.odist;
+      b.count = cnt * n1;
+      e = launch_split_bf16_pass(int(n2), dir, b, m, st);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+  std::string describe() const override {
+    std::ostringstream o;
+    o << "(c2c-split-bf16 n=" << n << " radix-16 DFT-matrix stages on tensor cores, 3-term bf16 splits";
+    if (n2) o << ", four-step " << n1 << "x" << n2 << " chunk=" << chunk;
+    o << ")";
+    return o.str();
+  }
+};
+
+static std::unique_ptr<Node> make_split_bf16(int64_t n, const Layout& lay, int dir, float scale, std::string* why) {
+  auto node = std::make_unique<SplitBf16Node>();
+  node->n = n;
+  node->dir = dir;
+  node->lay = lay;
+  if (n == 256 || n == 4096) {
+    node->n1 = n;
+  } else if (n == 65536 || n == (int64_t(1) << 20)) {
+    node->n1 = 256;
+    node->n2 = n / 256;
+  } else {
+    if (why) *why = "split-BF16 precision covers n = 256, 4096, 65536 and 2^20";
+    return nullptr;
+  }
+  auto stage_table = [&](int64_t nl, DevBuf& buf) {
+    std::vector<int> radices(nl == 256 ? 2 : 3, 16);
+    std::vector<float2> tw;
+    make_desc(int(nl), radices, tw);
+    return buf.upload(tw) == cudaSuccess;
+  };
+  const std::vector<uint32_t> mat = split_dft16(dir);
+  if (node->dftm.upload(mat) != cudaSuccess || !stage_table(node->n1, node->tw1) ||
+      (node->n2 && !stage_table(node->n2, node->tw2))) {
+    if (why) *why = "device allocation failed";
+    return nullptr;
+  }
+  const int64_t n1 = node->n1, n2 = node->n2;
+  if (!n2) {
+    node->p1 = FourStepLaunch{nullptr, nullptr, lay.howmany, 1, lay.idist, 0, lay.istride, lay.odist, 0,
+                              lay.ostride, split_bf16_pass_c(int(n1)), scale, node->tw1.as<float2>(),
+                              TwoLevel{nullptr, nullptr, 0, 1}};
+    return node;
+  }
+  const int64_t target = int64_t(env_int("PLFFT_B200_FS_CHUNK_MB", 256)) << 20;
+  node->chunk = std::max<int64_t>(1, std::min<int64_t>(lay.howmany, target / (n * 8)));
+  const int64_t L = int64_t(1) << ((ilog2(n) + 1) / 2);
+  std::vector<float2> lo(L), hi((n + L - 1) / L);
+  for (int64_t i = 0; i < L; ++i) lo[i] = root_f(i, n, -1);
+  for (size_t i = 0; i < hi.size(); ++i) hi[i] = root_f(int64_t(i) * L, n, -1);
+  if (node->lo.upload(lo) != cudaSuccess || node->hi.upload(hi) != cudaSuccess) {
+    if (why) *why = "device allocation failed";
+    return nullptr;
+  }
+  // pass 1: columns (member, n2 index), element k = n1 index, times W_n^{col k}
+  node->p1 = FourStepLaunch{nullptr, nullptr, 0, n2, lay.idist, lay.istride, n2 * lay.istride, n, 1, n2,
+                            split_bf16_pass_c(int(n1)), 1.0f, node->tw1.as<float2>(),
+                            TwoLevel{node->lo.as<float2>(), node->hi.as<float2>(), n, int(L)}};
+  // pass 2: rows (member, n1 index), element k = n2 index, written transposed
+  node->p2 = FourStepLaunch{nullptr, nullptr, 0, n1, n, n2, 1, lay.odist, lay.ostride, n1 * lay.ostride,
+                            split_bf16_pass_c(int(n2)), scale, node->tw2.as<float2>(), TwoLevel{nullptr, nullptr, 0, 1}};
+  return node;
+}
+
 std::unique_ptr<Node> make_c2c_node(int64_t n, const Layout& lay, int dir, float scale,
                                     int precision, std::string* why) {
-  (void)precision;
+  if (precision == 1) return make_split_bf16(n, lay, dir, scale, why);
   const bool unit = lay.istride == 1 && lay.ostride == 1;
   const bool interleaved = !unit && (lay.howmany > 1) &&
                            (std::llabs(lay.idist) < lay.istride || std::llabs(lay.odist) < lay.ostride);

@@ -34,36 +34,42 @@ struct qc {
 
 __device__ __forceinline__ int sat16(int v) { return min(max(v, -32768), 32767); }
 __device__ __forceinline__ int rshr(int v, int s) { return (v + (1 << (s - 1))) >> s; }
-// sqrdmulh by a constant k: |k| <= 32767 never overflows or saturates
+// sqrdmulh by a constant k, |k| <= 32767: never overflows or saturates
 template <int K>
 __device__ __forceinline__ int rdm(int a) {
-  if constexpr (K == -32768)
-    return min(-a, 32767);
-  else
-    return (2 * a * K + 32768) >> 16;
-}
-// two products accumulated in 32 bits (wrapping), then a rounding,
-// saturating narrow by 15 computed without overflow
-__device__ __forceinline__ int mac2(int a, int ka, int b, int kb) {
-  const int acc = int(unsigned(a) * unsigned(ka) + unsigned(b) * unsigned(kb));
-  return sat16((acc >> 15) + ((acc >> 14) & 1));
+  static_assert(K > -32768 && K <= 32767, "constant out of range");
+  return (2 * a * K + 32768) >> 16;
 }
 
+// Saturation: every codelet input is pre-shifted by log2(r), so |a| <= 2^15 / r
+// per component.  Interval analysis of each codelet (tests/test_q15.py::
+// test_q15_codelet_intermediates_never_saturate) shows that only the final
+// output additions can leave int16; intermediate sums, the sqrdmulh constant
+// products and the 32-bit MACs cannot.  Intermediates therefore use plain
+// integer arithmetic (identical results) and only outputs are clamped.
 __device__ __forceinline__ qc qadd(qc a, qc b) { return {sat16(a.re + b.re), sat16(a.im + b.im)}; }
 __device__ __forceinline__ qc qsub(qc a, qc b) { return {sat16(a.re - b.re), sat16(a.im - b.im)}; }
-__device__ __forceinline__ qc mul_pi(qc z) { return {rdm<-32768>(z.im), rdm<32767>(z.re)}; }
-__device__ __forceinline__ qc mul_mi(qc z) { return {rdm<32767>(z.im), rdm<-32768>(z.re)}; }
+__device__ __forceinline__ qc iadd(qc a, qc b) { return {a.re + b.re, a.im + b.im}; }
+__device__ __forceinline__ qc isub(qc a, qc b) { return {a.re - b.re, a.im - b.im}; }
+// sqrdmulh by -32768 is -a for the |a| < 2^15 that reach it
+__device__ __forceinline__ qc mul_pi(qc z) { return {-z.im, rdm<32767>(z.re)}; }
+__device__ __forceinline__ qc mul_mi(qc z) { return {rdm<32767>(z.im), -z.re}; }
+// 32-bit MAC + rounding shift by 15 of in-range operands (no wrap, no clamp)
+__device__ __forceinline__ int imac2(int a, int ka, int b, int kb) {
+  const int acc = a * ka + b * kb;
+  return (acc >> 15) + ((acc >> 14) & 1);
+}
 
 constexpr int kC8 = 23170, kC16 = 30273, kS16 = 12539;
 
 __device__ __forceinline__ qc mul_w8(qc z) {
-  return {mac2(z.re, kC8, rdm<kC8>(z.im), 32767), mac2(z.im, kC8, rdm<kC8>(z.re), -32768)};
+  return {imac2(z.re, kC8, rdm<kC8>(z.im), 32767), imac2(z.im, kC8, rdm<kC8>(z.re), -32768)};
 }
 __device__ __forceinline__ qc mul_w8_3(qc z) {
-  return {mac2(z.re, -kC8, rdm<-kC8>(z.im), -32768), mac2(z.im, -kC8, rdm<-kC8>(z.re), 32767)};
+  return {imac2(z.re, -kC8, rdm<-kC8>(z.im), -32768), imac2(z.im, -kC8, rdm<-kC8>(z.re), 32767)};
 }
 __device__ __forceinline__ qc mul_w(qc z, int wr, int wi) {
-  return {mac2(z.re, wr, z.im, -wi), mac2(z.im, wr, z.re, wi)};
+  return {imac2(z.re, wr, z.im, -wi), imac2(z.im, wr, z.re, wi)};
 }
 
 // ---- codelets on pre-scaled inputs, outputs in forward order ----
@@ -73,8 +79,8 @@ __device__ __forceinline__ void q_dft2(const qc* a, qc* y) {
 }
 
 __device__ __forceinline__ void q_dft4(const qc* a, qc* y) {
-  const qc s02 = qadd(a[0], a[2]), s13 = qadd(a[1], a[3]);
-  const qc d02 = qsub(a[0], a[2]), j13 = mul_pi(qsub(a[1], a[3]));
+  const qc s02 = iadd(a[0], a[2]), s13 = iadd(a[1], a[3]);
+  const qc d02 = isub(a[0], a[2]), j13 = mul_pi(isub(a[1], a[3]));
   y[0] = qadd(s02, s13);
   y[2] = qsub(s02, s13);
   y[1] = qsub(d02, j13);
@@ -85,20 +91,20 @@ __device__ __forceinline__ void q_dft8(const qc* a, qc* y) {
   qc p[4], m[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    p[k] = qadd(a[k], a[k + 4]);
-    m[k] = qsub(a[k], a[k + 4]);
+    p[k] = iadd(a[k], a[k + 4]);
+    m[k] = isub(a[k], a[k + 4]);
   }
-  const qc e0 = qadd(p[0], p[2]), e1 = qadd(p[1], p[3]);
+  const qc e0 = iadd(p[0], p[2]), e1 = iadd(p[1], p[3]);
   y[0] = qadd(e0, e1);
   y[4] = qsub(e0, e1);
-  const qc d = qsub(p[0], p[2]), jd = mul_pi(qsub(p[1], p[3]));
+  const qc d = isub(p[0], p[2]), jd = mul_pi(isub(p[1], p[3]));
   y[2] = qsub(d, jd);
   y[6] = qadd(d, jd);
-  const qc z = qadd(m[1], m[3]), w = qsub(m[1], m[3]);
+  const qc z = iadd(m[1], m[3]), w = isub(m[1], m[3]);
   const qc rd = {rdm<kC8>(w.re), rdm<kC8>(w.im)};
-  const qc x = {mac2(m[2].im, -32768, z.im, -kC8), mac2(m[2].re, 32767, z.re, kC8)};
-  const qc x2 = {mac2(m[2].im, -32768, z.im, kC8), mac2(m[2].re, 32767, z.re, -kC8)};
-  const qc u = qadd(m[0], rd), v = qsub(m[0], rd);
+  const qc x = {imac2(m[2].im, -32768, z.im, -kC8), imac2(m[2].re, 32767, z.re, kC8)};
+  const qc x2 = {imac2(m[2].im, -32768, z.im, kC8), imac2(m[2].re, 32767, z.re, -kC8)};
+  const qc u = iadd(m[0], rd), v = isub(m[0], rd);
   y[1] = qsub(u, x);
   y[7] = qadd(u, x);
   y[3] = qadd(v, x2);
@@ -109,42 +115,42 @@ __device__ __forceinline__ void q_dft16(const qc* a, qc* y) {
   qc p[8], m[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
-    p[k] = qadd(a[k], a[k + 8]);
-    m[k] = qsub(a[k], a[k + 8]);
+    p[k] = iadd(a[k], a[k + 8]);
+    m[k] = isub(a[k], a[k + 8]);
   }
-  const qc s04 = qadd(p[0], p[4]), s26 = qadd(p[2], p[6]);
-  const qc s15 = qadd(p[1], p[5]), s37 = qadd(p[3], p[7]);
-  const qc e0 = qadd(s04, s26), e1 = qadd(s15, s37);
+  const qc s04 = iadd(p[0], p[4]), s26 = iadd(p[2], p[6]);
+  const qc s15 = iadd(p[1], p[5]), s37 = iadd(p[3], p[7]);
+  const qc e0 = iadd(s04, s26), e1 = iadd(s15, s37);
   y[0] = qadd(e0, e1);
   y[8] = qsub(e0, e1);
-  const qc A = qsub(s04, s26), jB = mul_pi(qsub(s15, s37));
+  const qc A = isub(s04, s26), jB = mul_pi(isub(s15, s37));
   y[4] = qsub(A, jB);
   y[12] = qadd(A, jB);
-  const qc C = qsub(p[0], p[4]), jD = mul_pi(qsub(p[2], p[6]));
-  const qc kE = mul_w8(qsub(p[1], p[5])), kF = mul_w8_3(qsub(p[3], p[7]));
-  const qc g1 = qsub(C, jD), g2 = qadd(C, jD);
-  const qc h = qadd(kE, kF), h2 = mul_mi(qsub(kF, kE));
+  const qc C = isub(p[0], p[4]), jD = mul_pi(isub(p[2], p[6]));
+  const qc kE = mul_w8(isub(p[1], p[5])), kF = mul_w8_3(isub(p[3], p[7]));
+  const qc g1 = isub(C, jD), g2 = iadd(C, jD);
+  const qc h = iadd(kE, kF), h2 = mul_mi(isub(kF, kE));
   y[2] = qadd(g1, h);
   y[10] = qsub(g1, h);
   y[6] = qsub(g2, h2);
   y[14] = qadd(g2, h2);
   const qc j4 = mul_pi(m[4]);
-  const qc q = qsub(m[0], j4), q2 = qadd(m[0], j4);
+  const qc q = isub(m[0], j4), q2 = iadd(m[0], j4);
   const qc k2 = mul_w8(m[2]), k6 = mul_w8_3(m[6]);
-  const qc r = qadd(k2, k6), r2 = mul_mi(qsub(k6, k2));
+  const qc r = iadd(k2, k6), r2 = mul_mi(isub(k6, k2));
   const qc j5 = mul_pi(m[5]), j7 = mul_pi(m[7]);
-  const qc u = qsub(m[1], j5), u2 = qadd(m[1], j5);
-  const qc v = qsub(m[3], j7), v2 = qadd(m[3], j7);
+  const qc u = isub(m[1], j5), u2 = iadd(m[1], j5);
+  const qc v = isub(m[3], j7), v2 = iadd(m[3], j7);
   const qc l1 = mul_w(u, kC16, -kS16), l3 = mul_w(v, kS16, -kC16);
   const qc l3b = mul_w(u2, kS16, -kC16), l9 = mul_w(v2, -kC16, kS16);
-  const qc qr = qadd(q, r), qmr = qsub(q, r);
-  const qc ls = qadd(l1, l3), ld = mul_mi(qsub(l3, l1));
+  const qc qr = iadd(q, r), qmr = isub(q, r);
+  const qc ls = iadd(l1, l3), ld = mul_mi(isub(l3, l1));
   y[1] = qadd(qr, ls);
   y[9] = qsub(qr, ls);
   y[5] = qsub(qmr, ld);
   y[13] = qadd(qmr, ld);
-  const qc qa = qsub(q2, r2), qb = qadd(q2, r2);
-  const qc ls2 = qadd(l3b, l9), ld2 = mul_mi(qsub(l9, l3b));
+  const qc qa = isub(q2, r2), qb = iadd(q2, r2);
+  const qc ls2 = iadd(l3b, l9), ld2 = mul_mi(isub(l9, l3b));
   y[3] = qadd(qa, ls2);
   y[11] = qsub(qa, ls2);
   y[7] = qsub(qb, ld2);
@@ -242,7 +248,7 @@ __global__ void __launch_bounds__(256) q15_two_stage_kernel(const Q15Launch L) {
       } else {
         const int2 w = tw[15 * (j - 1) + (i - 1)];
         const qc cs = unpack(w.x), mc = unpack(w.y);  // (c, s), (-s, c)
-        a[i] = {mac2(s.re, cs.re, s.im, mc.re), mac2(s.re, cs.im, s.im, mc.im)};
+        a[i] = {imac2(s.re, cs.re, s.im, mc.re), imac2(s.re, cs.im, s.im, mc.im)};
       }
     }
     q_dft<16>(a, r);
