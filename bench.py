@@ -367,7 +367,7 @@ class Q15Workload(PlanWorkload):
     dtype = "int16"
 
     def __init__(self, name, desc, n, batch):
-        super().__init__(name, desc, "c2c", n, batch)
+        super().__init__(name, desc, "c2c", n, batch, profile="q15_two_stage_n256_b16384")
 
     def sizes(self):
         return self.n * self.batch * 4, self.n * self.batch * 4

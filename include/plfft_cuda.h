@@ -126,6 +126,15 @@ plfft_status_t plfft_cuda_c2c_execute_noalloc(const void *d_input,
                                              plfft_direction_t direction,
                                              void *stream);
 
+/* Wisdom: schedules chosen by the MEASURE / PATIENT / EXHAUSTIVE planners,
+ * one line per problem ("<problem key>\t<schedule>"), kept per process and,
+ * when the environment variable PLFFT_B200_WISDOM names a file, loaded from
+ * and appended to that file.  The reference keeps its wisdom private to the
+ * process (src/planner/wisdom.hpp:23-37); these persist it explicitly. */
+plfft_status_t plfft_cuda_wisdom_export(const char *path);
+plfft_status_t plfft_cuda_wisdom_import(const char *path);
+void plfft_cuda_wisdom_forget(void);
+
 #ifdef __cplusplus
 }
 #endif

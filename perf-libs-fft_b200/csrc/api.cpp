@@ -221,7 +221,8 @@ int plfft_cuda_plan_get_launch_count(const plfft_plan_t* plan) {
 
 plfft_status_t plfft_cuda_plan_describe(const plfft_plan_t* plan, char* buf, size_t len) {
   if (!plan || !buf) return PLFFT_NULL_ARGUMENT;
-  const std::string s = plan->p.root->describe();
+  std::string s = plan->p.root->describe();
+  if (!plan->p.tune_note.empty()) s += " [" + plan->p.tune_note + "]";
   if (len == 0) return PLFFT_INVALID_ARGUMENT;
   std::snprintf(buf, len, "%s", s.c_str());
   return PLFFT_OK;

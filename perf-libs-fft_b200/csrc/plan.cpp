@@ -174,6 +174,11 @@ struct C2CRegNode : Node {
 // ---------------------------------------------------------------------------
 // static power-of-two C2C node (bulk-copy staged, compile-time radices)
 // ---------------------------------------------------------------------------
+// explicit launch shape (0 / -1: planner default or environment override)
+struct Pow2Params {
+  int e = 0, ring = -1, g = 0, gp = -1;
+};
+
 struct C2CPow2Node : Node {
   Pow2Launch base{};
   int n = 0, e = 0, dir = -1;
@@ -190,7 +195,10 @@ struct C2CPow2Node : Node {
   }
   std::string describe() const override {
     std::ostringstream o;
-    o << "(c2c-pow2 n=" << n << " e=" << e << " g=" << base.g << (base.ring ? " ring" : "") << " bulk-copy)";
+    o << "(c2c-pow2 n=" << n << " e=" << e << " g=" << base.g;
+    if (base.ring == 1) o << " ring";
+    if (base.ring >= 2) o << " group-ring" << base.ring << " gp=" << base.gp;
+    o << " bulk-copy)";
     return o.str();
   }
 };
@@ -202,8 +210,9 @@ static int pow2_default_e(int64_t n) {
   return 32;
 }
 
-static std::unique_ptr<Node> make_pow2(int64_t n, const Layout& lay, int dir, float scale, std::string* why) {
-  int e = env_int("PLFFT_B200_POW2_E", pow2_default_e(n));
+static std::unique_ptr<Node> make_pow2(int64_t n, const Layout& lay, int dir, float scale, std::string* why,
+                                       const Pow2Params& pp = Pow2Params{}) {
+  int e = pp.e ? pp.e : env_int("PLFFT_B200_POW2_E", pow2_default_e(n));
   if (!pow2_supported(int(n), e)) e = pow2_default_e(n);
   if (!pow2_supported(int(n), e)) return nullptr;
   auto node = std::make_unique<C2CPow2Node>();
@@ -228,7 +237,7 @@ static std::unique_ptr<Node> make_pow2(int64_t n, const Layout& lay, int dir, fl
     return nullptr;
   }
   const int t = int(n / e);
-  int g = std::max(1, env_int("PLFFT_B200_POW2_G", std::max(1, 64 / t)));
+  int g = std::max(1, pp.g ? pp.g : env_int("PLFFT_B200_POW2_G", std::max(1, 64 / t)));
   const int maxthr = e <= 16 ? 512 : 256;
   while (g > 1 && (g * t > maxthr || pow2_smem_bytes(int(n), g) > 200 * 1024)) g /= 2;
   node->base.howmany = lay.howmany;
@@ -241,8 +250,8 @@ static std::unique_ptr<Node> make_pow2(int64_t n, const Layout& lay, int dir, fl
   node->base.err = node->err.as<int>();
   // CTA ring of g transforms per CTA: measured best for n = 1024 (4.07 TB/s
   // against 3.51 for the warp-group rings at batch 4096)
-  node->base.ring = env_int("PLFFT_B200_POW2_RING", 1);
-  node->base.gp = std::max(0, env_int("PLFFT_B200_POW2_GP", 0));
+  node->base.ring = pp.ring >= 0 ? pp.ring : env_int("PLFFT_B200_POW2_RING", 1);
+  node->base.gp = std::max(0, pp.gp >= 0 ? pp.gp : env_int("PLFFT_B200_POW2_GP", 0));
   return node;
 }
 
@@ -435,7 +444,8 @@ static int fourstep_c(int nl) {
   return c;
 }
 
-static std::unique_ptr<Node> make_four_step_pow2(int64_t n, const Layout& lay, int dir, float scale) {
+static std::unique_ptr<Node> make_four_step_pow2(int64_t n, const Layout& lay, int dir, float scale,
+                                                 int c_override = 0, int chunk_mb = 0) {
   if (!is_pow2(n) || std::getenv("PLFFT_B200_NO_FS_POW2")) return nullptr;
   int b = ilog2(n);
   const int64_t n1 = int64_t(1) << (b / 2), n2 = n / n1;
@@ -446,7 +456,7 @@ static std::unique_ptr<Node> make_four_step_pow2(int64_t n, const Layout& lay, i
   node->n2 = n2;
   node->dir = dir;
   node->lay = lay;
-  const int64_t target = int64_t(env_int("PLFFT_B200_FS_CHUNK_MB", 256)) << 20;
+  const int64_t target = int64_t(chunk_mb ? chunk_mb : env_int("PLFFT_B200_FS_CHUNK_MB", 256)) << 20;
   node->chunk = std::max<int64_t>(1, std::min<int64_t>(lay.howmany, target / (n * 8)));
   auto stage_table = [&](int64_t nl, DevBuf& buf) {
     const int e = fourstep_pass_e(int(nl));
@@ -471,11 +481,12 @@ static std::unique_ptr<Node> make_four_step_pow2(int64_t n, const Layout& lay, i
   if (node->lo.upload(lo) != cudaSuccess || node->hi.upload(hi) != cudaSuccess) return nullptr;
   // pass 1: sub-transform g = (member, column n2 index), element k = n1 index
   node->p1 = FourStepLaunch{nullptr, nullptr, 0, n2, lay.idist, lay.istride, n2 * lay.istride, n, 1, n2,
-                            fourstep_c(int(n1)), 1.0f, node->tw1.as<float2>(),
+                            c_override ? c_override : fourstep_c(int(n1)), 1.0f, node->tw1.as<float2>(),
                             TwoLevel{node->lo.as<float2>(), node->hi.as<float2>(), n, int(L)}};
   // pass 2: sub-transform g = (member, row k1), element k = n2 index
   node->p2 = FourStepLaunch{nullptr, nullptr, 0, n1, n, n2, 1, lay.odist, lay.ostride, n1 * lay.ostride,
-                            fourstep_c(int(n2)), scale, node->tw2.as<float2>(), TwoLevel{nullptr, nullptr, 0, 1}};
+                            c_override ? c_override : fourstep_c(int(n2)), scale, node->tw2.as<float2>(),
+                            TwoLevel{nullptr, nullptr, 0, 1}};
   return node;
 }
 
@@ -695,6 +706,61 @@ std::unique_ptr<Node> make_c2c_node(int64_t n, const Layout& lay, int dir, float
   if (auto fs = make_four_step_pow2(n, lay, dir, scale)) return fs;
   if (is_smooth(n)) return make_four_step(n, lay, dir, scale, why);
   return make_conv_node(n, lay, dir, scale, why);
+}
+
+// Alternative schedules for the same C2C problem, default first (the
+// autotuner times them).  level 1: launch shapes of the chosen kernel
+// family; level 2: also other kernel families and radix sizes; level 3:
+// also four-step CTA shapes and chunk sizes.
+std::vector<std::unique_ptr<Node>> make_c2c_candidates(int64_t n, const Layout& lay, int dir, float scale,
+                                                       int precision, int level) {
+  std::vector<std::unique_ptr<Node>> out;
+  std::string why;
+  if (auto d = make_c2c_node(n, lay, dir, scale, precision, &why)) out.push_back(std::move(d));
+  if (precision != 0 || out.empty()) return out;
+  const bool unit = lay.istride == 1 && lay.ostride == 1;
+  if (unit && is_pow2(n) && n >= 64 && n <= 8192) {
+    std::vector<int> es{pow2_default_e(n)};
+    if (level >= 2)
+      for (int e : {16, 32})
+        if (e != es[0] && pow2_supported(int(n), e)) es.push_back(e);
+    for (int e : es) {
+      const int t = int(n / e);
+      for (int ring : {0, 1, 3}) {
+        for (int g : {1, 2, 4, 8}) {
+          if (ring == 3 && g != 1) continue;  // warp-group rings size themselves
+          if (g * t > (e <= 16 ? 512 : 256)) continue;
+          Pow2Params pp;
+          pp.e = e;
+          pp.ring = ring;
+          pp.g = g;
+          if (auto c = make_pow2(n, lay, dir, scale, &why, pp)) out.push_back(std::move(c));
+        }
+      }
+    }
+  }
+  if (level >= 2 && n <= kMaxOnChip && is_smooth(n)) {
+    const bool interleaved = !unit && (lay.howmany > 1) &&
+                             (std::llabs(lay.idist) < lay.istride || std::llabs(lay.odist) < lay.ostride);
+    Addr ia{lay.idist, 0, lay.istride, 1};
+    Addr oa{lay.odist, 0, lay.ostride, 1};
+    if (auto t = make_tile(n, lay.howmany, ia, oa, dir, scale, interleaved, &why)) out.push_back(std::move(t));
+  }
+  if (is_pow2(n) && n > 8192) {
+    for (int c : {4, 8, 16})
+      for (int mb : {64, 256, 1024}) {
+        if (level < 3 && mb != 256) continue;
+        if (auto f = make_four_step_pow2(n, lay, dir, scale, c, mb)) out.push_back(std::move(f));
+      }
+  }
+  // drop duplicates of the default (same description)
+  std::vector<std::unique_ptr<Node>> uniq;
+  for (auto& c : out) {
+    bool dup = false;
+    for (auto& u : uniq) dup = dup || u->describe() == c->describe();
+    if (!dup) uniq.push_back(std::move(c));
+  }
+  return uniq;
 }
 
 PlanData::~PlanData() {

@@ -118,6 +118,16 @@ int64_t four_step_split(int64_t n);
 std::unique_ptr<Node> make_c2c_node(int64_t n, const Layout& lay, int dir, float scale,
                                     int precision, std::string* why);
 
+// Alternative C2C schedules for the autotuner, the default first; level 1-3
+// widens the search (launch shapes, kernel families, four-step shapes).
+std::vector<std::unique_ptr<Node>> make_c2c_candidates(int64_t n, const Layout& lay, int dir, float scale,
+                                                       int precision, int level);
+
+// Plan-time autotuning for rigor MEASURE/PATIENT/EXHAUSTIVE (autotune.cpp):
+// times the candidates and remembers the winner in wisdom; note receives
+// "wisdom" or "autotuned k/m candidates".
+std::unique_ptr<Node> autotune_c2c(const ConfigData& c, const Layout& lay, std::string* why, std::string* note);
+
 // Q0.15 fixed-point C2C node (plan_q15.cpp); nullptr (with why) if unsupported.
 std::unique_ptr<Node> make_q15_node(int64_t n, const Layout& lay, int dir, std::string* why);
 
@@ -163,6 +173,7 @@ struct PlanData {
   int64_t in_elems = 0, out_elems = 0;  // span of one execute, elements
   int in_bytes = 0, out_bytes = 0;      // element sizes
   bool out_dense = false;               // the output span is fully written
+  std::string tune_note;                // how the schedule was chosen (rigor > ESTIMATE)
   ~PlanData();
 };
 

@@ -44,7 +44,10 @@ plfft_status_t build_plan(PlanData& p, std::string* why) {
   if (c.data_type == PLFFT_DATA_TYPE_FP32) {
     switch (c.kind) {
       case TKind::C2C:
-        p.root = make_c2c_node(c.n, lay, c.payload, scale, c.precision, why);
+        if (c.rigor == PLFFT_ESTIMATE)
+          p.root = make_c2c_node(c.n, lay, c.payload, scale, c.precision, why);
+        else
+          p.root = autotune_c2c(c, lay, why, &p.tune_note);
         break;
       case TKind::R2C:
         p.root = make_real_fused_node(FR_R2C, c.n, lay, scale);

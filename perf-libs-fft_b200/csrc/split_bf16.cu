@@ -47,9 +47,10 @@ __device__ __forceinline__ void split3(float a, float b, uint32_t& w0, uint32_t&
   w2 = pack_bf16(a2, b2);
 }
 
-// D += A (16x16 bf16, row) * B (16x8 bf16, col), FP32 accumulate
+// D += A (16x16 bf16, row) * B (16x8 bf16, col), FP32 accumulate (no side
+// effects, so not volatile: the compiler may interleave independent MMAs)
 __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-  asm volatile(
+  asm(
       "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
       "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
       : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
@@ -91,46 +92,48 @@ __device__ __forceinline__ void sb_stage(float2* tile, int pitch, int ns, const 
                                          const SbA& A, int warp, int g, int t) {
   constexpr int J = NL / 16;  // columns per sub-transform
   float acc[NT][2][4];
+  // n-tiles in pairs: the two tiles' MMAs alternate, so consecutive MMAs
+  // accumulate into different registers
 #pragma unroll
-  for (int it = 0; it < NT; ++it) {
-    const int v = (warp * NT + it) * 8 + g;  // this thread's B column
-    const int c = v / J, j = v - c * J;
-    const float2* x = tile + c * pitch;
-    const int r = j & (ns - 1);
-    // u_q for q in {2t, 2t+1, 2t+8, 2t+9}, twiddled by W_{16 ns}^{r q}
-    float2 u[4];
+  for (int it0 = 0; it0 < NT; it0 += 2) {
+    uint32_t b[2][3][2][2];  // [tile][split][k-step][reg]
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const int q = 2 * t + (e & 1) + (e >> 1) * 8;
-      float2 val = x[spad(j + q * J)];
-      if (ns > 1 && q > 0) val = twmul<DIR>(val, tw[(q - 1) * ns + r]);
-      u[e] = val;
-    }
-    // B operands: k-step 0 = real parts, k-step 1 = imaginary parts
-    uint32_t b[3][2][2];
-    split3(u[0].x, u[1].x, b[0][0][0], b[1][0][0], b[2][0][0]);
-    split3(u[2].x, u[3].x, b[0][0][1], b[1][0][1], b[2][0][1]);
-    split3(u[0].y, u[1].y, b[0][1][0], b[1][1][0], b[2][1][0]);
-    split3(u[2].y, u[3].y, b[0][1][1], b[1][1][1], b[2][1][1]);
+    for (int p = 0; p < 2; ++p) {
+      const int v = (warp * NT + it0 + p) * 8 + g;  // this thread's B column
+      const int c = v / J, j = v - c * J;
+      const float2* x = tile + c * pitch;
+      const int r = j & (ns - 1);
+      // u_q for q in {2t, 2t+1, 2t+8, 2t+9}, twiddled by W_{16 ns}^{r q}
+      float2 u[4];
 #pragma unroll
-    for (int mt = 0; mt < 2; ++mt) {
-#pragma unroll
-      for (int i = 0; i < 4; ++i) acc[it][mt][i] = 0.f;
-      // smallest products first
-#pragma unroll
-      for (int ks = 0; ks < 2; ++ks) {
-        mma_bf16(acc[it][mt], A.r[2][mt][ks], b[0][ks][0], b[0][ks][1]);
-        mma_bf16(acc[it][mt], A.r[1][mt][ks], b[1][ks][0], b[1][ks][1]);
-        mma_bf16(acc[it][mt], A.r[0][mt][ks], b[2][ks][0], b[2][ks][1]);
+      for (int e = 0; e < 4; ++e) {
+        const int q = 2 * t + (e & 1) + (e >> 1) * 8;
+        float2 val = x[spad(j + q * J)];
+        if (ns > 1 && q > 0) val = twmul<DIR>(val, tw[(q - 1) * ns + r]);
+        u[e] = val;
       }
+      // B operands: k-step 0 = real parts, k-step 1 = imaginary parts
+      split3(u[0].x, u[1].x, b[p][0][0][0], b[p][1][0][0], b[p][2][0][0]);
+      split3(u[2].x, u[3].x, b[p][0][0][1], b[p][1][0][1], b[p][2][0][1]);
+      split3(u[0].y, u[1].y, b[p][0][1][0], b[p][1][1][0], b[p][2][1][0]);
+      split3(u[2].y, u[3].y, b[p][0][1][1], b[p][1][1][1], b[p][2][1][1]);
 #pragma unroll
-      for (int ks = 0; ks < 2; ++ks) {
-        mma_bf16(acc[it][mt], A.r[1][mt][ks], b[0][ks][0], b[0][ks][1]);
-        mma_bf16(acc[it][mt], A.r[0][mt][ks], b[1][ks][0], b[1][ks][1]);
-      }
+      for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-      for (int ks = 0; ks < 2; ++ks) mma_bf16(acc[it][mt], A.r[0][mt][ks], b[0][ks][0], b[0][ks][1]);
+        for (int i = 0; i < 4; ++i) acc[it0 + p][mt][i] = 0.f;
     }
+    // products W_sa x_sb with sa + sb <= 2, smallest first
+    constexpr int kSa[6] = {2, 1, 0, 1, 0, 0};
+    constexpr int kSb[6] = {0, 1, 2, 0, 1, 0};
+#pragma unroll
+    for (int term = 0; term < 6; ++term)
+#pragma unroll
+      for (int ks = 0; ks < 2; ++ks)
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+          for (int p = 0; p < 2; ++p)
+            mma_bf16(acc[it0 + p][mt], A.r[kSa[term]][mt][ks], b[p][kSb[term]][ks][0], b[p][kSb[term]][ks][1]);
   }
   __syncthreads();  // every column of this stage has been read
 #pragma unroll

@@ -141,6 +141,9 @@ _SIGS = [
     ("plfft_cuda_group_get_launch_count", _INT, [_P]),
     ("plfft_cuda_group_describe", _INT, [_P, ctypes.c_char_p, ctypes.c_size_t]),
     ("plfft_cuda_group_destroy", None, [_P]),
+    ("plfft_cuda_wisdom_export", _INT, [ctypes.c_char_p]),
+    ("plfft_cuda_wisdom_import", _INT, [ctypes.c_char_p]),
+    ("plfft_cuda_wisdom_forget", None, []),
 ]
 
 # symbols bound when the library exports them (added by later components)
@@ -374,6 +377,21 @@ def make_plan(kind, n, howmany=1, istride=1, idist=None, ostride=1, odist=None, 
         return Plan(cfg)
     finally:
         cfg.destroy()
+
+
+# ---------------------------------------------------------------------------
+# wisdom of the MEASURE / PATIENT / EXHAUSTIVE planners
+# ---------------------------------------------------------------------------
+def wisdom_export(path):
+    _check(lib().plfft_cuda_wisdom_export(os.fsencode(path)), "wisdom_export")
+
+
+def wisdom_import(path):
+    _check(lib().plfft_cuda_wisdom_import(os.fsencode(path)), "wisdom_import")
+
+
+def wisdom_forget():
+    lib().plfft_cuda_wisdom_forget()
 
 
 # ---------------------------------------------------------------------------

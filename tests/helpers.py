@@ -38,7 +38,7 @@ def gather(buf, howmany, dist, n, stride):
 
 
 def c2c_case(n, howmany=1, istride=1, idist=None, ostride=1, odist=None, direction=-1, seed=0,
-             alias=False, scale=1.0, host=False, method="auto"):
+             alias=False, scale=1.0, host=False, method="auto", rigor=None):
     """Run a C2C plan on seeded data; return (got, ref) logical arrays."""
     import torch
 
@@ -49,7 +49,8 @@ def c2c_case(n, howmany=1, istride=1, idist=None, ostride=1, odist=None, directi
     x = seeded_complex(nin, seed)
     xin = x.copy()
     plan = plfft.make_plan("c2c", n, howmany, istride, idist, ostride, odist, direction=direction,
-                           alias=plfft.IoAlias.MAY_ALIAS if alias else plfft.IoAlias.NO_ALIAS, scale=scale)
+                           alias=plfft.IoAlias.MAY_ALIAS if alias else plfft.IoAlias.NO_ALIAS, scale=scale,
+                           rigor=plfft.Rigor.ESTIMATE if rigor is None else rigor)
     if host:
         out = np.zeros(nout, np.complex64) if not alias else x
         plan.execute(x.ctypes.data, out.ctypes.data)
