@@ -22,7 +22,7 @@ namespace plfft_b200 {
 
 
 template <int N, int E, int DIR>
-__global__ void __launch_bounds__(pow2_max_threads<E>()) c2c_pow2_kernel(const Pow2Launch L) {
+__global__ void __launch_bounds__(pow2_max_threads<E>(), pow2_min_blocks<E>()) c2c_pow2_kernel(const Pow2Launch L) {
   using P = P2<N, E>;
   constexpr int T = P::T;
   extern __shared__ __align__(128) unsigned char smraw[];
@@ -110,36 +110,40 @@ __global__ void __launch_bounds__(pow2_max_threads<E>()) c2c_pow2_kernel(const P
   }
 }
 
-// Persistent variant: each CTA owns a ring of kRing buffer slots and walks
-// the groups blockIdx.x, blockIdx.x + gridDim.x, ...  The bulk loads of the
-// next two groups are in flight while the current one is transformed, and
-// each result leaves through an asynchronous bulk store.
-constexpr int kRing = 3;
+// Persistent variant: each CTA owns a ring of R = L.slots buffer slots and
+// walks the groups blockIdx.x, blockIdx.x + gridDim.x, ...  The bulk loads
+// of the next R-1 groups are in flight while the current one is
+// transformed, and each result leaves through an asynchronous bulk store.
+// TWS: the stage twiddles are copied to shared memory once per CTA.
+constexpr int kMaxSlots = 8;
 
-template <int N, int E, int DIR>
-__global__ void __launch_bounds__(pow2_max_threads<E>()) c2c_pow2_ring_kernel(const Pow2Launch L) {
+template <int N, int E, int DIR, bool TWS>
+__global__ void __launch_bounds__(pow2_max_threads<E>(), pow2_min_blocks<E>()) c2c_pow2_ring_kernel(const Pow2Launch L) {
   using P = P2<N, E>;
   constexpr int T = P::T;
   constexpr int PITCH = (spad_len_c(N) + 1) & ~1;
   extern __shared__ __align__(128) unsigned char smraw[];
-  __shared__ uint64_t bar[kRing];
+  __shared__ uint64_t bar[kMaxSlots];
   const int G = L.g;
+  const int R = L.slots;
   const int64_t ngroups = (L.howmany + G - 1) / G;
   const int grp = threadIdx.x / T;
   const int t = threadIdx.x - grp * T;
   float2* const ring = reinterpret_cast<float2*>(smraw);
+  float2* const tws = ring + R * G * PITCH;
+  const float2* tw = TWS ? tws : L.tw;
 
   auto group_of = [&](int k) { return int64_t(blockIdx.x) + int64_t(k) * gridDim.x; };
   auto count_of = [&](int64_t g) {
     const int64_t r = L.howmany - g * G;
     return r < G ? int(r) : G;
   };
-  auto slot = [&](int k) { return ring + (k % kRing) * G * PITCH; };
+  auto slot = [&](int k) { return ring + (k % R) * G * PITCH; };
   auto issue = [&](int k) {  // thread 0 only
     const int64_t g = group_of(k);
     if (g >= ngroups) return;
     const int cnt = count_of(g);
-    uint64_t* b = &bar[k % kRing];
+    uint64_t* b = &bar[k % R];
     mbar_arrive_expect_tx(b, uint32_t(cnt) * N * 8u);
     float2* dst = slot(k);
     for (int c = 0; c < cnt; ++c) bulk_g2s(dst + c * PITCH, L.in + (g * G + c) * L.idist, N * 8u, b);
@@ -152,20 +156,25 @@ __global__ void __launch_bounds__(pow2_max_threads<E>()) c2c_pow2_ring_kernel(co
   };
 
   if (threadIdx.x == 0) {
-    for (int b = 0; b < kRing; ++b) mbar_init(&bar[b], 1);
+    for (int b = 0; b < R; ++b) mbar_init(&bar[b], 1);
     mbar_fence_init();
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    issue(0);
-    issue(1);
+  // with direct stores a slot is free again right after its transform, so
+  // all R slots hold loads in flight; with bulk stores one slot drains
+  const int ahead = L.dstore ? R : R - 1;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < ahead; ++k) issue(k);
+  if constexpr (TWS) {
+    for (int i = threadIdx.x; i < L.tw_len; i += blockDim.x) tws[i] = L.tw[i];
+    __syncthreads();
   }
   for (int k = 0; group_of(k) < ngroups; ++k) {
     const int64_t g = group_of(k);
     const int cnt = count_of(g);
     const bool live = grp < cnt;
     float2* mine = slot(k) + grp * PITCH;
-    const bool ok = mbar_wait_bounded(&bar[k % kRing], uint32_t(k / kRing) & 1u);
+    const bool ok = mbar_wait_bounded(&bar[k % R], uint32_t(k / R) & 1u);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) atomicExch(L.err, 1);
       break;
@@ -178,12 +187,26 @@ __global__ void __launch_bounds__(pow2_max_threads<E>()) c2c_pow2_ring_kernel(co
 #pragma unroll
       for (int q = 0; q < E; ++q) v[q] = make_float2(0.f, 0.f);
     }
-    st_bfly<T, E, P::radix(0), 1, 0, DIR>(v, t, L.tw);
-    Stages<N, E, DIR, 1>::run(v, t, mine, L.tw, sync);
+    st_bfly<T, E, P::radix(0), 1, 0, DIR, TWS>(v, t, tw);
+    Stages<N, E, DIR, 1, TWS>::run(v, t, mine, tw, sync);
     const float s = L.scale;
     if (s != 1.f) {
 #pragma unroll
       for (int q = 0; q < E; ++q) v[q] = cscale(v[q], s);
+    }
+    if (L.dstore) {
+      // coalesced stores from registers; the slot is refilled at once
+      if (live) {
+        float2* dst = L.out + (g * G + grp) * L.odist;
+#pragma unroll
+        for (int q = 0; q < E; ++q) dst[t + T * q] = v[q];
+      }
+      __syncthreads();  // every read of this slot is done
+      if (threadIdx.x == 0) {
+        fence_proxy_async();
+        issue(k + R);
+      }
+      continue;
     }
     sync();
     if (live) {
@@ -197,7 +220,7 @@ __global__ void __launch_bounds__(pow2_max_threads<E>()) c2c_pow2_ring_kernel(co
       for (int c = 0; c < cnt; ++c) bulk_s2g(L.out + (g * G + c) * L.odist, src + c * PITCH, N * 8u);
       bulk_commit();
       bulk_wait_read_but1();  // the slot of group k-1 is free again
-      issue(k + 2);
+      issue(k + R - 1);
     }
   }
   if (threadIdx.x == 0) bulk_wait_read_all();
@@ -360,8 +383,9 @@ static cudaError_t run_pow2(const Pow2Launch& L, cudaStream_t st) {
     }
   }
   if (L.tma_in && L.tma_out && L.ring) {
-    auto* k = c2c_pow2_ring_kernel<N, E, DIR>;
-    const int smem = kRing * pow2_smem_bytes(N, L.g);
+    if (L.slots < 2 || L.slots > kMaxSlots) return cudaErrorInvalidValue;
+    auto* k = L.tws ? c2c_pow2_ring_kernel<N, E, DIR, true> : c2c_pow2_ring_kernel<N, E, DIR, false>;
+    const int smem = L.slots * pow2_smem_bytes(N, L.g) + (L.tws ? ((L.tw_len + 1) & ~1) * 8 : 0);
     if (smem > 32 * 1024) {  // leave room for static shared memory
       cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
       if (e != cudaSuccess) return e;

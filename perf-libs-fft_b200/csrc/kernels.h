@@ -67,6 +67,9 @@ struct Pow2Launch {
   int tw_len;  // entries in tw
   int tma_in, tma_out;
   int ring;  // 0 one-shot CTAs, 1 CTA ring, 2/3 warp-group rings (slots)
+  int slots;  // CTA ring: buffer slots (2..8), loads run slots-1 groups ahead
+  int tws;    // CTA ring: stage twiddles copied to shared memory
+  int dstore; // CTA ring: results stored from registers (no bulk store)
   int gp;    // warp-group kernel: groups per CTA (0 = as many as fit)  // persistent ring-buffered variant
   int* err;  // set to 1 if a bounded device wait ran out
 };

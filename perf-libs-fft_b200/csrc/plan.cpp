@@ -176,7 +176,7 @@ struct C2CRegNode : Node {
 // ---------------------------------------------------------------------------
 // explicit launch shape (0 / -1: planner default or environment override)
 struct Pow2Params {
-  int e = 0, ring = -1, g = 0, gp = -1;
+  int e = 0, ring = -1, g = 0, gp = -1, slots = 0, tws = -1, dstore = -1;
 };
 
 struct C2CPow2Node : Node {
@@ -196,7 +196,8 @@ struct C2CPow2Node : Node {
   std::string describe() const override {
     std::ostringstream o;
     o << "(c2c-pow2 n=" << n << " e=" << e << " g=" << base.g;
-    if (base.ring == 1) o << " ring";
+    if (base.ring == 1)
+      o << " ring slots=" << base.slots << (base.tws ? " tw-smem" : "") << (base.dstore ? " direct-store" : "");
     if (base.ring >= 2) o << " group-ring" << base.ring << " gp=" << base.gp;
     o << " bulk-copy)";
     return o.str();
@@ -237,7 +238,7 @@ static std::unique_ptr<Node> make_pow2(int64_t n, const Layout& lay, int dir, fl
     return nullptr;
   }
   const int t = int(n / e);
-  int g = std::max(1, pp.g ? pp.g : env_int("PLFFT_B200_POW2_G", std::max(1, 64 / t)));
+  int g = std::max(1, pp.g ? pp.g : env_int("PLFFT_B200_POW2_G", std::max(1, 32 / t)));
   const int maxthr = e <= 16 ? 512 : 256;
   while (g > 1 && (g * t > maxthr || pow2_smem_bytes(int(n), g) > 200 * 1024)) g /= 2;
   node->base.howmany = lay.howmany;
@@ -248,10 +249,18 @@ static std::unique_ptr<Node> make_pow2(int64_t n, const Layout& lay, int dir, fl
   node->base.tw = node->tw.as<float2>();
   node->base.tw_len = int(tw.size());
   node->base.err = node->err.as<int>();
-  // CTA ring of g transforms per CTA: measured best for n = 1024 (4.07 TB/s
-  // against 3.51 for the warp-group rings at batch 4096)
+  // CTA ring, one transform per CTA for n = 1024 (g = 32 / T), 3 slots:
+  // measured best at batch 4096 (4.09 TB/s; deeper rings, twiddles in
+  // shared memory, register stores and the warp-group rings were slower)
   node->base.ring = pp.ring >= 0 ? pp.ring : env_int("PLFFT_B200_POW2_RING", 1);
   node->base.gp = std::max(0, pp.gp >= 0 ? pp.gp : env_int("PLFFT_B200_POW2_GP", 0));
+  node->base.slots = std::min(8, std::max(2, pp.slots ? pp.slots : env_int("PLFFT_B200_POW2_SLOTS", 3)));
+  node->base.tws = pp.tws >= 0 ? pp.tws : env_int("PLFFT_B200_POW2_TWS", 0);
+  node->base.dstore = pp.dstore >= 0 ? pp.dstore : env_int("PLFFT_B200_POW2_DS", 0);
+  // the ring's slots must fit in shared memory
+  while (node->base.slots > 2 &&
+         node->base.slots * pow2_smem_bytes(int(n), g) + node->base.tws * int(tw.size() + 1) * 8 > 200 * 1024)
+    --node->base.slots;
   return node;
 }
 
@@ -765,6 +774,8 @@ std::vector<std::unique_ptr<Node>> make_c2c_candidates(int64_t n, const Layout& 
 
 PlanData::~PlanData() {
   if (stream) cudaStreamDestroy(stream);
+  for (auto& st : pipe_st)
+    if (st) cudaStreamDestroy(st);
 }
 
 }  // namespace plfft_b200

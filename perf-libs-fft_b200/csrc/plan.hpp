@@ -174,6 +174,15 @@ struct PlanData {
   int in_bytes = 0, out_bytes = 0;      // element sizes
   bool out_dense = false;               // the output span is fully written
   std::string tune_note;                // how the schedule was chosen (rigor > ESTIMATE)
+  int64_t nin = 0, nout = 0;            // logical elements per member
+  // host-buffer pipeline (plfft_plan_execute on host pointers): the batch in
+  // chunks whose copies and kernels overlap across streams; built on first use
+  static constexpr int kPipeStreams = 3;
+  mutable bool pipe_built = false;
+  mutable int64_t pipe_per = 0;  // members per chunk, 0 = no pipeline
+  mutable std::unique_ptr<Node> pipe_node, pipe_tail;
+  mutable cudaStream_t pipe_st[kPipeStreams] = {};
+  mutable DevBuf pipe_ws[kPipeStreams];
   ~PlanData();
 };
 

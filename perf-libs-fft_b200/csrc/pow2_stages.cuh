@@ -81,5 +81,9 @@ struct Stages {
 
 template <int E>
 constexpr int pow2_max_threads() { return E <= 16 ? 512 : 256; }
+// minimum resident blocks for __launch_bounds__: caps E=32 kernels at 128
+// registers (they fit without spilling), which doubles the warps per SM
+template <int E>
+constexpr int pow2_min_blocks() { return E <= 16 ? 1 : 2; }
 
 }  // namespace plfft_b200

@@ -138,3 +138,31 @@ def test_c2c_output_guard_band():
     idx = (np.arange(hm)[:, None] * od + np.arange(n)[None, :] * os_).ravel()
     mask[idx] = False
     assert np.all(yc[mask] == np.complex64(sentinel))
+
+
+@pytest.mark.parametrize("kind,n,howmany", [("c2c", 1024, 2501), ("r2c", 4096, 1500), ("c2r", 4096, 1500)])
+def test_host_buffers_pipelined_chunks(kind, n, howmany):
+    """plfft_plan_execute on large host batches runs as overlapped chunks
+    (copies and kernels on several streams), with a shorter last chunk."""
+    import plfft
+
+    rng = np.random.default_rng(21)
+    h = n // 2 + 1
+    plan = plfft.make_plan(kind, n, howmany)
+    if kind == "c2c":
+        x = (rng.uniform(-1, 1, (howmany, n)) + 1j * rng.uniform(-1, 1, (howmany, n))).astype(np.complex64)
+        y = np.zeros_like(x)
+        plan.execute(x.ctypes.data, y.ctypes.data)
+        ref = oracle.c2c(x.astype(np.complex128), -1, method="fft")
+    elif kind == "r2c":
+        x = rng.uniform(-1, 1, (howmany, n)).astype(np.float32)
+        y = np.zeros((howmany, h), np.complex64)
+        plan.execute(x.ctypes.data, y.ctypes.data)
+        ref = oracle.r2c(x.astype(np.float64), method="fft")
+    else:
+        spec = oracle.r2c(rng.uniform(-1, 1, (howmany, n)), method="fft")
+        x = spec.astype(np.complex64)
+        y = np.zeros((howmany, n), np.float32)
+        plan.execute(x.ctypes.data, y.ctypes.data)
+        ref = oracle.c2r(x.astype(np.complex128), n, method="fft")
+    assert oracle.rel_l2(y, ref) <= oracle.fp32_tol(n), plan.describe()
