@@ -244,6 +244,21 @@ int split_bf16_pass_c(int nl);
 cudaError_t launch_split_bf16_pass(int nl, int dir, const FourStepLaunch& L, const uint32_t* dftm,
                                    cudaStream_t st);
 
+// Single-pass four-step for n = 256 x 256 on an 8-CTA cluster
+// (fourstep_cluster.cu); any strides, members idist/odist apart.
+struct FourStepClusterLaunch {
+  const float2* in;
+  float2* out;
+  int64_t howmany;
+  int64_t istride, idist, ostride, odist;
+  float scale;
+  const float2* tw;  // stage twiddles of the 256-point FFT
+  TwoLevel tw2;      // W_n^{c k1}
+};
+int fourstep_cluster_smem();
+int fourstep_cluster_capacity();
+cudaError_t launch_fourstep_cluster(int dir, const FourStepClusterLaunch& L, int max_clusters, cudaStream_t st);
+
 // kernel entry points (c2c.cu)
 cudaError_t launch_c2c_reg(int e, int dir, const RegLaunch& L, cudaStream_t st);
 cudaError_t launch_c2c_tile(int maxe, int dir, const TileLaunch& L, cudaStream_t st);

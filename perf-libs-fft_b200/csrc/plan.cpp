@@ -499,6 +499,46 @@ static std::unique_ptr<Node> make_four_step_pow2(int64_t n, const Layout& lay, i
   return node;
 }
 
+// single-pass four-step for n = 65536 on an 8-CTA cluster (fourstep_cluster.cu)
+struct C2CFourStepClusterNode : Node {
+  int dir = -1, clusters = 1;
+  FourStepClusterLaunch base{};
+  DevBuf tw, lo, hi;
+  cudaError_t run(const void* in, void* out, void*, cudaStream_t st) const override {
+    FourStepClusterLaunch L = base;
+    L.in = static_cast<const float2*>(in);
+    L.out = static_cast<float2*>(out);
+    return launch_fourstep_cluster(dir, L, clusters, st);
+  }
+  std::string describe() const override {
+    std::ostringstream o;
+    o << "(c2c-four-step-cluster n=65536 256x256 one pass, 8-CTA clusters x" << clusters << ")";
+    return o.str();
+  }
+};
+
+static std::unique_ptr<Node> make_four_step_cluster(int64_t n, const Layout& lay, int dir, float scale) {
+  if (n != 65536) return nullptr;
+  const int cap = fourstep_cluster_capacity();
+  if (cap < 1) return nullptr;
+  auto node = std::make_unique<C2CFourStepClusterNode>();
+  node->dir = dir;
+  node->clusters = cap;
+  std::vector<float2> tw;
+  make_desc(256, std::vector<int>{16, 16}, tw);
+  const int64_t L = 256;
+  std::vector<float2> lo(L), hi(n / L);
+  for (int64_t i = 0; i < L; ++i) lo[i] = root_f(i, n, -1);
+  for (int64_t i = 0; i < n / L; ++i) hi[i] = root_f(i * L, n, -1);
+  if (node->tw.upload(tw) != cudaSuccess || node->lo.upload(lo) != cudaSuccess ||
+      node->hi.upload(hi) != cudaSuccess)
+    return nullptr;
+  node->base = FourStepClusterLaunch{nullptr, nullptr, lay.howmany, lay.istride, lay.idist, lay.ostride, lay.odist,
+                                     scale, node->tw.as<float2>(),
+                                     TwoLevel{node->lo.as<float2>(), node->hi.as<float2>(), n, int(L)}};
+  return node;
+}
+
 static std::unique_ptr<Node> make_four_step(int64_t n, const Layout& lay, int dir, float scale,
                                             std::string* why) {
   const int64_t best = four_step_split(n);
@@ -712,6 +752,8 @@ std::unique_ptr<Node> make_c2c_node(int64_t n, const Layout& lay, int dir, float
     auto t = make_tile(n, lay.howmany, ia, oa, dir, scale, interleaved, why);
     if (t) return t;
   }
+  if (std::getenv("PLFFT_B200_CLUSTER"))
+    if (auto fc = make_four_step_cluster(n, lay, dir, scale)) return fc;
   if (auto fs = make_four_step_pow2(n, lay, dir, scale)) return fs;
   if (is_smooth(n)) return make_four_step(n, lay, dir, scale, why);
   return make_conv_node(n, lay, dir, scale, why);
@@ -756,6 +798,10 @@ std::vector<std::unique_ptr<Node>> make_c2c_candidates(int64_t n, const Layout& 
     if (auto t = make_tile(n, lay.howmany, ia, oa, dir, scale, interleaved, &why)) out.push_back(std::move(t));
   }
   if (is_pow2(n) && n > 8192) {
+    // the one-pass cluster form (one HBM round trip, but latency-bound at
+    // 8 warps per SM: 1.13 TB/s against 1.8 for two passes at 2^16 x 1024)
+    if (level >= 2)
+      if (auto f = make_four_step_cluster(n, lay, dir, scale)) out.push_back(std::move(f));
     for (int c : {4, 8, 16})
       for (int mb : {64, 256, 1024}) {
         if (level < 3 && mb != 256) continue;

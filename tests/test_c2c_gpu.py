@@ -166,3 +166,26 @@ def test_host_buffers_pipelined_chunks(kind, n, howmany):
         plan.execute(x.ctypes.data, y.ctypes.data)
         ref = oracle.c2r(x.astype(np.complex128), n, method="fft")
     assert oracle.rel_l2(y, ref) <= oracle.fp32_tol(n), plan.describe()
+
+
+@pytest.fixture
+def cluster_form(monkeypatch):
+    """Select the one-pass cluster form of n = 65536 (an autotuner candidate)."""
+    monkeypatch.setenv("PLFFT_B200_CLUSTER", "1")
+
+
+@pytest.mark.parametrize("direction", [-1, 1])
+@pytest.mark.parametrize("layout", [(41, 1, None, 1, None), (3, 2, 1, 3, 1)])
+def test_c2c_cluster_four_step(cluster_form, direction, layout):
+    """n = 65536 in one pass on 8-CTA clusters: more members than resident
+    clusters (the clusters loop), and interleaved strided members."""
+    hm, is_, id_, os_, od = layout
+    got, ref, plan = c2c_case(65536, hm, is_, id_, os_, od, direction=direction, seed=4, method="fft")
+    assert "cluster" in plan.describe(), plan.describe()
+    assert oracle.rel_l2(got, ref) <= oracle.fp32_tol(65536), plan.describe()
+
+
+def test_c2c_cluster_four_step_in_place(cluster_form):
+    got, ref, plan = c2c_case(65536, 5, alias=True, seed=8, method="fft")
+    assert "cluster" in plan.describe(), plan.describe()
+    assert oracle.rel_l2(got, ref) <= oracle.fp32_tol(65536), plan.describe()
