@@ -54,6 +54,12 @@ __global__ void __launch_bounds__(512) fourstep_pass_kernel(const FourStepLaunch
       const int c = f / NL, k = f - c * NL;
       cp_async8(slots + c * PITCH + k, L.in + ibase[c] + k);
     }
+  } else if ((cnt & (cnt - 1)) == 0) {  // full power-of-two tile: shifts, no division
+    const int sh = __ffs(cnt) - 1;
+    for (int f = threadIdx.x; f < total; f += blockDim.x) {
+      const int k = f >> sh, c = f & (cnt - 1);
+      cp_async8(slots + c * PITCH + k, L.in + ibase[c] + int64_t(k) * L.iks);
+    }
   } else {
     for (int f = threadIdx.x; f < total; f += blockDim.x) {
       const int k = f / cnt, c = f - k * cnt;
@@ -92,6 +98,12 @@ __global__ void __launch_bounds__(512) fourstep_pass_kernel(const FourStepLaunch
     for (int f = threadIdx.x; f < total; f += blockDim.x) {
       const int c = f / NL, k = f - c * NL;
       L.out[obase[c] + k] = slots[c * PITCH + k];
+    }
+  } else if ((cnt & (cnt - 1)) == 0) {
+    const int sh = __ffs(cnt) - 1;
+    for (int f = threadIdx.x; f < total; f += blockDim.x) {
+      const int k = f >> sh, c = f & (cnt - 1);
+      L.out[obase[c] + int64_t(k) * L.oks] = slots[c * PITCH + k];
     }
   } else {
     for (int f = threadIdx.x; f < total; f += blockDim.x) {
