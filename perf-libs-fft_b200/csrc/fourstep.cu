@@ -81,10 +81,18 @@ __global__ void __launch_bounds__(512) fourstep_pass_kernel(const FourStepLaunch
   st_bfly<T, E, P::radix(0), 1, 0, DIR>(v, t, L.tw);
   Stages<NL, E, DIR, 1>::run(v, t, mine, L.tw, sync);
   if (L.post.n != 0 && grp < cnt) {
+    // W_n^{col k}, k = t + T q: a table lookup every fourth q and a product
+    // with W_n^{col T} in between (at most three extra roundings, a quarter
+    // of the table loads)
     const uint32_t col = uint32_t(colv[grp]);
     const int lshift = __ffs(L.post.l) - 1;
+    const float2 step = fs_two_level(L.post, col * uint32_t(T), lshift);
+    float2 w = make_float2(1.f, 0.f);
 #pragma unroll
-    for (int q = 0; q < E; ++q) v[q] = twmul<DIR>(v[q], fs_two_level(L.post, col * uint32_t(t + T * q), lshift));
+    for (int q = 0; q < E; ++q) {
+      w = (q & 3) == 0 ? fs_two_level(L.post, col * uint32_t(t + T * q), lshift) : cmul(w, step);
+      v[q] = twmul<DIR>(v[q], w);
+    }
   }
   if (L.scale != 1.f) {
 #pragma unroll
