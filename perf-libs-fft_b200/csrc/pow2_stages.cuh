@@ -34,14 +34,26 @@ __device__ __forceinline__ void st_bfly(float2 (&v)[E], int t, const float2* __r
       const int j = t + T * m;
       const int r = j & (NS - 1);
       const float2* w = tw + TWOFF + r;
-#pragma unroll
-      for (int i = 1; i < R; ++i) {
-        float2 wi;
+      // W^{r i} for i = 1..R-1: for R >= 16 a table entry every fourth i
+      // and products with W^r in between (at most three extra roundings,
+      // a quarter of the loads); small radices load every entry
+      auto load = [&](int i) {
         if constexpr (TWS)
-          wi = w[(i - 1) * NS];
+          return w[(i - 1) * NS];
         else
-          wi = __ldg(w + (i - 1) * NS);
-        x[i] = twmul<DIR>(x[i], wi);
+          return __ldg(w + (i - 1) * NS);
+      };
+      if constexpr (R >= 16) {
+        const float2 w1 = load(1);
+        float2 wi = w1;
+#pragma unroll
+        for (int i = 1; i < R; ++i) {
+          if (i > 1) wi = (i & 3) == 1 ? load(i) : cmul(wi, w1);
+          x[i] = twmul<DIR>(x[i], wi);
+        }
+      } else {
+#pragma unroll
+        for (int i = 1; i < R; ++i) x[i] = twmul<DIR>(x[i], load(i));
       }
     }
     dft<R, DIR>(x);
