@@ -200,6 +200,7 @@ struct RealFusedLaunch {
   const float2* post;  // W_N^k, k = 0..M
   const float2* rot;   // exp(-i pi k / 2N), k = 0..M
   int pairs_in, pairs_out;  // real data may be moved as aligned float pairs
+  int e;                    // elements per thread of the length-M FFT
 };
 bool real_fused_supported(int m);
 int real_fused_e(int m);

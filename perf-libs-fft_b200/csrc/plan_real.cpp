@@ -132,7 +132,7 @@ struct RealFusedNode : Node {
   std::string describe() const override {
     static const char* names[] = {"r2c", "c2r", "dct2", "dst2"};
     std::ostringstream o;
-    o << "(" << names[kind] << "-fused n=" << 2 * m << " m=" << m << " e=" << real_fused_e(m) << " g=" << base.g
+    o << "(" << names[kind] << "-fused n=" << 2 * m << " m=" << m << " e=" << base.e << " g=" << base.g
       << ")";
     return o.str();
   }
@@ -144,7 +144,9 @@ std::unique_ptr<Node> make_real_fused_node(int kind, int64_t n, const Layout& la
   if (n % 2 || !real_fused_supported(int(n / 2)) || lay.istride != 1 || lay.ostride != 1) return nullptr;
   if (std::getenv("PLFFT_B200_NO_FUSED_REAL")) return nullptr;
   const int m = int(n / 2);
-  const int e = real_fused_e(m);
+  int e = real_fused_e(m);
+  if (const char* v = std::getenv("PLFFT_B200_RF_E"))  // launch-shape experiments
+    if (m == 512 && std::atoi(v) == 32) e = 32;
   std::vector<int> radices;
   int rest = m, ke = 0;
   while (rest % e == 0 && rest > 1) {
@@ -176,6 +178,8 @@ std::unique_ptr<Node> make_real_fused_node(int kind, int64_t n, const Layout& la
   node->base.idist = lay.idist;
   node->base.odist = lay.odist;
   node->base.g = std::max(1, 128 / t);
+  if (const char* v = std::getenv("PLFFT_B200_RF_G")) node->base.g = std::max(1, std::atoi(v));
+  node->base.e = e;
   node->base.scale = scale;
   node->base.tw = node->tab.as<float2>();
   node->base.post = node->tab.as<float2>() + post_off;

@@ -22,7 +22,8 @@ struct P2 {
 
 // TWS: the twiddle table lives in shared memory (plain loads) instead of
 // global memory (read-only cache loads)
-template <int T, int E, int R, int NS, int TWOFF, int DIR, bool TWS = false>
+// RMIN: smallest radix whose twiddles use the lookup-every-fourth recurrence
+template <int T, int E, int R, int NS, int TWOFF, int DIR, bool TWS = false, int RMIN = 16>
 __device__ __forceinline__ void st_bfly(float2 (&v)[E], int t, const float2* __restrict__ tw) {
   constexpr int M = E / R;
 #pragma unroll
@@ -43,7 +44,7 @@ __device__ __forceinline__ void st_bfly(float2 (&v)[E], int t, const float2* __r
         else
           return __ldg(w + (i - 1) * NS);
       };
-      if constexpr (R >= 16) {
+      if constexpr (R >= RMIN) {
         const float2 w1 = load(1);
         float2 wi = w1;
 #pragma unroll
@@ -74,7 +75,7 @@ __device__ __forceinline__ void st_scatter(const float2 (&v)[E], int t, float2* 
   }
 }
 
-template <int N, int E, int DIR, int S, bool TWS = false>
+template <int N, int E, int DIR, int S, bool TWS = false, int RMIN = 16>
 struct Stages {
   using P = P2<N, E>;
   template <class Sync>
@@ -85,8 +86,8 @@ struct Stages {
       sync();
 #pragma unroll
       for (int q = 0; q < E; ++q) v[q] = xb[spad(t + P::T * q)];
-      st_bfly<P::T, E, P::radix(S), P::ns(S), P::twoff(S), DIR, TWS>(v, t, tw);
-      Stages<N, E, DIR, S + 1, TWS>::run(v, t, xb, tw, sync);
+      st_bfly<P::T, E, P::radix(S), P::ns(S), P::twoff(S), DIR, TWS, RMIN>(v, t, tw);
+      Stages<N, E, DIR, S + 1, TWS, RMIN>::run(v, t, xb, tw, sync);
     }
   }
 };
