@@ -139,7 +139,7 @@ class PlanWorkload(Workload):
         return self.plan.describe()
 
     def cpu_sample(self, threads):
-        """FP64 oracle on a bounded sample; returns (seconds per sample, sample bytes, text)."""
+        """FP64 oracle on a bounded sample; returns (run one sample, sample bytes, text)."""
         import numpy as np
 
         import oracle
@@ -173,15 +173,9 @@ class PlanWorkload(Workload):
         else:
             x = rng.uniform(-1, 1, (m, self.n))
             fn = lambda: oracle.r2r(x, self.r2r, threads=threads)  # noqa: E731
-        fn()
-        reps = 3
-        t0 = time.perf_counter()
-        for _ in range(reps):
-            fn()
-        dt = (time.perf_counter() - t0) / reps
         frac = m / self.batch
         how = "direct sums" if (self.kind == "r2r" and self.r2r not in ("DCT_2", "DST_2")) else "mixed-radix FFT"
-        return dt, self.algo_bytes() * frac, f"{m} of {self.batch} transforms, FP64 {how} (oracle/)"
+        return fn, self.algo_bytes() * frac, f"{m} of {self.batch} transforms, FP64 {how} (oracle/)"
 
 
 class RoundTripWorkload(PlanWorkload):
@@ -332,11 +326,11 @@ class GroupedWorkload(Workload):
 
         pick = self.lengths[:: max(1, len(self.lengths) // 200)]
         xs = [np.random.default_rng(int(n)).standard_normal(n) + 0j for n in pick]
-        t0 = time.perf_counter()
-        for x in xs:
-            oracle.c2c(x[None], -1, method="fft", threads=threads)
-        dt = time.perf_counter() - t0
-        return dt, 16 * float(np.sum(pick)), f"{len(pick)} of {self.count} transforms, FP64 FFT (oracle/)"
+
+        def fn():
+            for x in xs:
+                oracle.c2c(x[None], -1, method="fft", threads=threads)
+        return fn, 16 * float(np.sum(pick)), f"{len(pick)} of {self.count} transforms, FP64 FFT (oracle/)"
 
 
 class AdjointWorkload(PlanWorkload):
@@ -416,13 +410,8 @@ class Q15Workload(PlanWorkload):
         m = min(self.batch, 4096)
         rng = np.random.default_rng(0)
         x = rng.integers(-(1 << 14), 1 << 14, (m, self.n, 2)).astype(np.int16)
-        oracle.q15_c2c(x[:16], -1)
-        reps = 3
-        t0 = time.perf_counter()
-        for _ in range(reps):
-            oracle.q15_c2c(x, -1)
-        dt = (time.perf_counter() - t0) / reps
-        return dt, self.algo_bytes() * m / self.batch, f"{m} of {self.batch} transforms, bit-exact Q0.15 C restatement (oracle/q15.c, 1 thread)"
+        return (lambda: oracle.q15_c2c(x, -1), self.algo_bytes() * m / self.batch,
+                f"{m} of {self.batch} transforms, bit-exact Q0.15 C restatement (oracle/q15.c, 1 thread)")
 
 
 def make_workload(name):
@@ -532,12 +521,49 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(w):
+def _calibrate(fn):
+    """Seconds of one sample after a warm-up call."""
+    fn()
+    t0 = time.perf_counter()
+    fn()
+    return max(time.perf_counter() - t0, 1e-6)
+
+
+def cpu_baseline(w, target_s=10.0):
+    """The CPU oracle on repetitions of a bounded sample, about target_s seconds."""
     import oracle
 
     threads = oracle.max_threads()
-    dt, sbytes, text = w.cpu_sample(threads)
-    return {"value": sbytes / dt / 1e9, "unit": "GB/s", "cores": threads, "kind": "port", "sample": text}
+    fn, sbytes, text = w.cpu_sample(threads)
+    reps = max(1, min(100000, int(target_s / _calibrate(fn))))
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        fn()
+    dt = (time.perf_counter() - t0) / reps
+    return {"value": sbytes / dt / 1e9, "unit": "GB/s", "cores": threads, "kind": "port",
+            "sample": f"{text}, {reps} repetitions ({reps * dt:.1f} s)"}
+
+
+def reference_arm(w, steps, warmup, budget_s=120.0):
+    """The reference's CPU path (the oracle port: the reference cannot be
+    built here) timed as `steps` steps of a bounded sample after `warmup`
+    untimed ones; the whole run stays within about budget_s seconds."""
+    import oracle
+
+    threads = oracle.max_threads()
+    fn, sbytes, text = w.cpu_sample(threads)
+    one = _calibrate(fn)
+    per_step = min(10.0, max(0.05, budget_s / max(1, steps + warmup)))
+    reps = max(1, int(per_step / one))
+    for _ in range(warmup * reps):
+        fn()
+    t0 = time.perf_counter()
+    for _ in range(steps * reps):
+        fn()
+    dt = time.perf_counter() - t0
+    value = steps * reps * sbytes / dt / 1e9
+    return value, {"value": value, "unit": "GB/s", "cores": threads, "kind": "port",
+                   "sample": f"{text}, {reps} repetitions per step"}, dt * 1e3 / steps
 
 
 # --------------------------------------------------------------------------
@@ -564,12 +590,14 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        cpu = cpu_baseline(w)
-        line = {"metric": f"{w.name} GB/s (algorithmic bytes)", "value": cpu["value"], "unit": "GB/s",
-                "impl": "reference", "n_gpus": args.gpus, "steps": 1, "warmup": 1,
+        steps = args.steps if args.steps is not None else 10
+        value, cpu, ms = reference_arm(w, steps, args.warmup)
+        line = {"metric": f"{w.name} GB/s (algorithmic bytes)", "value": value, "unit": "GB/s",
+                "impl": "reference", "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
+                "ms_per_step": ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64" if w.dtype == "f32" else w.dtype,
                 "data": "synthetic (seeded U[-1,1))", "config": w.config(), "cpu_baseline": cpu,
-                "e2e": {"value": cpu["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
 
