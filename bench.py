@@ -432,7 +432,8 @@ def make_workload(name):
                                                        "c2c", 1 << 20, 64, precision=1),
         "c2c_n64k_b1024_split_bf16": lambda: PlanWorkload("c2c_n64k_b1024_split_bf16",
                                                           "C2C N=2^16 batch=1024, split-BF16 tensor-core stages",
-                                                          "c2c", 1 << 16, 1024, precision=1),
+                                                          "c2c", 1 << 16, 1024, precision=1,
+                                                          profile="split_bf16_pass_n64k_b1024"),
         "grouped_4000": lambda: GroupedWorkload(),
         "q15_n256_b16384": lambda: Q15Workload("q15_n256_b16384", "C2C Q0.15 forward N=256 batch=16384", 256, 16384),
         "diff_r2c_n8192_b1024": lambda: AdjointWorkload(),
