@@ -260,6 +260,13 @@ int fourstep_cluster_smem();
 int fourstep_cluster_capacity();
 cudaError_t launch_fourstep_cluster(int dir, const FourStepClusterLaunch& L, int max_clusters, cudaStream_t st);
 
+// FP16 data type (half_io.cu): strided binary16 <-> dense FP32 chunk;
+// comps = 1 (real) or 2 (complex) scalars per element.
+cudaError_t launch_half_gather(const void* src, float* dense, int64_t m0, int64_t cnt, int64_t n, int64_t stride,
+                               int64_t dist, int comps, cudaStream_t st);
+cudaError_t launch_half_scatter(const float* dense, void* dst, int64_t m0, int64_t cnt, int64_t n, int64_t stride,
+                                int64_t dist, int comps, cudaStream_t st);
+
 // kernel entry points (c2c.cu)
 cudaError_t launch_c2c_reg(int e, int dir, const RegLaunch& L, cudaStream_t st);
 cudaError_t launch_c2c_tile(int maxe, int dir, const TileLaunch& L, cudaStream_t st);

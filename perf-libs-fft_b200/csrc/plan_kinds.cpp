@@ -35,6 +35,8 @@ static int64_t span(int64_t howmany, int64_t dist, int64_t n, int64_t stride) {
   return (howmany - 1) * (howmany > 1 ? dist : 0) + (n - 1) * stride + 1;
 }
 
+static std::unique_ptr<Node> make_half_node(const ConfigData& c, const Layout& lay, std::string* why);
+
 // device schedule for configuration c over the batch layout lay; tune:
 // allow plan-time autotuning (rigor above ESTIMATE)
 static std::unique_ptr<Node> make_root(const ConfigData& c, const Layout& lay, bool tune, std::string* why,
@@ -67,6 +69,12 @@ static std::unique_ptr<Node> make_root(const ConfigData& c, const Layout& lay, b
         break;
       }
     }
+  } else if (c.data_type == PLFFT_DATA_TYPE_FP16) {
+    if (c.precision != 0) {
+      if (why) *why = "the split-BF16 precision mode takes FP32 data";
+    } else {
+      root = make_half_node(c, lay, why);
+    }
   } else if (c.data_type == PLFFT_DATA_TYPE_Q15 && c.kind == TKind::C2C) {
     if (c.scale != 1.0) {
       if (why) *why = "fixed-point transforms are scaled by 1/n and take no extra scale";
@@ -81,6 +89,69 @@ static std::unique_ptr<Node> make_root(const ConfigData& c, const Layout& lay, b
     if (why) *why = "data type not supported on the device path";
   }
   return root;
+}
+
+// FP16 (binary16) data: widen a chunk of members into dense FP32, run the
+// FP32 schedule for that chunk, round the results back to binary16.
+struct HalfIoNode : Node {
+  std::unique_ptr<Node> inner, inner_tail;  // FP32 schedules: full chunk, last chunk
+  Layout user{};
+  int64_t chunk = 1, nin = 0, nout = 0;
+  int icomps = 1, ocomps = 1;
+  size_t in_bytes() const { return size_t(chunk * nin * icomps) * sizeof(float); }
+  size_t out_bytes() const { return size_t(chunk * nout * ocomps) * sizeof(float); }
+  size_t inner_ws() const {
+    return std::max(inner->workspace(), inner_tail ? inner_tail->workspace() : size_t(0));
+  }
+  size_t workspace() const override { return (in_bytes() + 255) / 256 * 256 + (out_bytes() + 255) / 256 * 256 + inner_ws(); }
+  int launches() const override {
+    const int64_t chunks = (user.howmany + chunk - 1) / chunk;
+    return int(chunks) * (2 + inner->launches());
+  }
+  cudaError_t run(const void* in, void* out, void* ws, cudaStream_t st) const override {
+    auto* base = static_cast<unsigned char*>(ws);
+    float* din = reinterpret_cast<float*>(base);
+    float* dout = reinterpret_cast<float*>(base + (in_bytes() + 255) / 256 * 256);
+    void* iws = base + (in_bytes() + 255) / 256 * 256 + (out_bytes() + 255) / 256 * 256;
+    for (int64_t m0 = 0; m0 < user.howmany; m0 += chunk) {
+      const int64_t cnt = std::min(chunk, user.howmany - m0);
+      const Node& node = cnt == chunk ? *inner : *inner_tail;
+      cudaError_t e = launch_half_gather(in, din, m0, cnt, nin, user.istride, user.idist, icomps, st);
+      if (e == cudaSuccess) e = node.run(din, dout, iws, st);
+      if (e == cudaSuccess) e = launch_half_scatter(dout, out, m0, cnt, nout, user.ostride, user.odist, ocomps, st);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+  std::string describe() const override {
+    return "(fp16 io: binary16 <-> FP32 chunks of " + std::to_string(chunk) + ") + " + inner->describe();
+  }
+};
+
+static std::unique_ptr<Node> make_half_node(const ConfigData& c, const Layout& lay, std::string* why) {
+  int64_t nin = 0, nout = 0;
+  bool ic = false, oc = false;
+  io_counts(c, nin, nout, ic, oc);
+  auto node = std::make_unique<HalfIoNode>();
+  node->user = lay;
+  node->nin = nin;
+  node->nout = nout;
+  node->icomps = ic ? 2 : 1;
+  node->ocomps = oc ? 2 : 1;
+  // in-place: one chunk, so no member's input is overwritten before it is read
+  const int64_t per = (nin * node->icomps + nout * node->ocomps) * int64_t(sizeof(float));
+  node->chunk = c.alias == PLFFT_IO_MAY_ALIAS
+                    ? c.howmany
+                    : std::max<int64_t>(1, std::min<int64_t>(c.howmany, (int64_t(256) << 20) / per));
+  ConfigData c32 = c;
+  c32.data_type = PLFFT_DATA_TYPE_FP32;
+  c32.alias = PLFFT_IO_NO_ALIAS;
+  const int64_t tail = c.howmany - (c.howmany - 1) / node->chunk * node->chunk;
+  std::string note;
+  node->inner = make_root(c32, Layout{node->chunk, 1, nin, 1, nout}, false, why, &note);
+  if (tail != node->chunk) node->inner_tail = make_root(c32, Layout{tail, 1, nin, 1, nout}, false, why, &note);
+  if (!node->inner || (tail != node->chunk && !node->inner_tail)) return nullptr;
+  return node;
 }
 
 plfft_status_t build_plan(PlanData& p, std::string* why) {
