@@ -267,6 +267,43 @@ cudaError_t launch_half_gather(const void* src, float* dense, int64_t m0, int64_
 cudaError_t launch_half_scatter(const float* dense, void* dst, int64_t m0, int64_t cnt, int64_t n, int64_t stride,
                                 int64_t dist, int comps, cudaStream_t st);
 
+// FP64 data type (fp64.cu)
+struct F64Stage {
+  int radix, ns, tw_off, om_off;
+};
+struct F64Desc {
+  int n, nstages;
+  F64Stage st[24];
+};
+struct TwoLevel64 {
+  const double2* lo;
+  const double2* hi;
+  int64_t n;  // 0: no four-step twiddle
+  int64_t l;
+};
+struct F64TileLaunch {
+  const double2* in;
+  double2* out;
+  int64_t ntr;     // transforms (one per CTA)
+  Addr ia, oa;     // element addressing, as the FP32 tile launch
+  double scale;
+  F64Desc desc;    // n and stages (direct kernel: n only)
+  const double2* tw;     // stage twiddles (direct kernel: W_n^m, m < n)
+  const double2* omega;  // exp(-2 pi i q / R) for each stage radix
+  TwoLevel64 post;       // W_N^{col k} on the outputs when post.n != 0
+};
+struct F64RealLaunch {
+  const void* in;
+  void* out;
+  double2* work;  // [cnt][n] complex
+  int64_t n, istride, idist, ostride, odist;
+  int c2r;
+  double scale;
+};
+int fp64_tile_smem(int n);
+cudaError_t launch_fp64_tile(int dir, bool direct, const F64TileLaunch& L, cudaStream_t st);
+cudaError_t launch_fp64_real(bool pre, const F64RealLaunch& L, int64_t m0, int64_t cnt, cudaStream_t st);
+
 // kernel entry points (c2c.cu)
 cudaError_t launch_c2c_reg(int e, int dir, const RegLaunch& L, cudaStream_t st);
 cudaError_t launch_c2c_tile(int maxe, int dir, const TileLaunch& L, cudaStream_t st);

@@ -128,6 +128,11 @@ std::vector<std::unique_ptr<Node>> make_c2c_candidates(int64_t n, const Layout& 
 // "wisdom" or "autotuned k/m candidates".
 std::unique_ptr<Node> autotune_c2c(const ConfigData& c, const Layout& lay, std::string* why, std::string* note);
 
+// FP64 nodes (plan_fp64.cpp): kind 0 C2C, 1 R2C, 2 C2R; nullptr (with why)
+// when the length or kind has no FP64 schedule.
+std::unique_ptr<Node> make_fp64_node(int kind, int64_t n, const Layout& lay, int dir, double scale,
+                                     std::string* why);
+
 // Q0.15 fixed-point C2C node (plan_q15.cpp); nullptr (with why) if unsupported.
 std::unique_ptr<Node> make_q15_node(int64_t n, const Layout& lay, int dir, std::string* why);
 

@@ -69,6 +69,13 @@ static std::unique_ptr<Node> make_root(const ConfigData& c, const Layout& lay, b
         break;
       }
     }
+  } else if (c.data_type == PLFFT_DATA_TYPE_FP64) {
+    if (c.precision != 0) {
+      if (why) *why = "the split-BF16 precision mode takes FP32 data";
+    } else {
+      root = make_fp64_node(int(c.kind), c.n, lay, c.kind == TKind::C2C ? c.payload : (c.kind == TKind::R2C ? -1 : 1),
+                            c.scale, why);
+    }
   } else if (c.data_type == PLFFT_DATA_TYPE_FP16) {
     if (c.precision != 0) {
       if (why) *why = "the split-BF16 precision mode takes FP32 data";
