@@ -60,10 +60,9 @@ __device__ __forceinline__ void finish_real(float2 (&v)[E], const RealFusedLaunc
     for (int q = 0; q < E; ++q) mine[t + T * q] = v[q];
     sync();
     if (!live) return;
-    // k = t + T*j for j < E covers 0..M-1; thread 0 also takes k = M
-    for (int j = 0; j <= E; ++j) {
-      const int k = j < E ? t + T * j : M;
-      if (j == E && t != 0) break;
+    // k = t + T*j for j < E covers 0..M-1 (unrolled, so the table loads
+    // of all j are in flight together); thread 0 also takes k = M
+    auto out_k = [&](int k) {
       const float2 V = real_split(mine, k, M, L.post);
       if constexpr (KIND == FR_R2C) {
         static_cast<float2*>(L.out)[b * L.odist + k] = cscale(V, s);
@@ -79,7 +78,10 @@ __device__ __forceinline__ void finish_real(float2 (&v)[E], const RealFusedLaunc
           if (k > 0 && k < M) y[k - 1] = ynk;
         }
       }
-    }
+    };
+#pragma unroll
+    for (int j = 0; j < E; ++j) out_k(t + T * j);
+    if (t == 0) out_k(M);
   }
 }
 
