@@ -25,6 +25,7 @@
 #include <stdint.h>
 
 #include "kernels.h"
+#include "ptx.cuh"
 
 namespace plfft_b200 {
 
@@ -214,11 +215,13 @@ __global__ void __launch_bounds__(256) q15_two_stage_kernel(const Q15Launch L) {
   const int64_t left = L.howmany - b0;
   const int cnt = left < G ? int(left) : G;
   for (int i = threadIdx.x; i < 15 * (M - 1); i += blockDim.x) tw[i] = L.tw[i];
-  // stage the members (each thread: consecutive elements across members)
+  // stage the members (each thread: consecutive elements across members),
+  // asynchronous copies so that all of a thread's loads are in flight
   for (int f = threadIdx.x; f < cnt * N; f += blockDim.x) {
     const int g = f / N, k = f - g * N;
-    tile[g * PITCH + q15_pos(k)] = L.in[(b0 + g) * L.idist + int64_t(k) * L.istride];
+    cp_async4(tile + g * PITCH + q15_pos(k), L.in + (b0 + g) * L.idist + int64_t(k) * L.istride);
   }
+  cp_async_wait_all();
   __syncthreads();
   const int g = threadIdx.x >> 4, c = threadIdx.x & 15;
   int* mine = tile + g * PITCH;

@@ -144,6 +144,7 @@ __global__ void __launch_bounds__(pow2_max_threads<E>()) real_fused_kernel(const
     // Makhoul-permuted pairs
     float* xs = reinterpret_cast<float*>(mine);
     const float* x = static_cast<const float*>(L.in) + (live ? b * L.idist : 0);
+#pragma unroll
     for (int f = t; f < N; f += T) {
       float val = live ? x[f] : 0.f;
       if constexpr (KIND == FR_DST2) val = (f & 1) ? -val : val;
