@@ -99,31 +99,45 @@ __device__ void run_tile(const GTask& T, const GroupPhase& P, float2* sm) {
   const float2* in = P.bases[T.in_buf] + T.in_off;
   float2* out = P.bases[T.out_buf] + T.out_off;
   const float2* xin = P.bases[T.aux_buf] + T.aux_off;
+  // element f = (c, k) walks the tile with the fast index along the
+  // contiguous dimension; (c, k) is carried from one iteration to the next
+  // (one division per tile, not per element) and the loop is unrolled so
+  // that several loads are in flight per thread
   const bool kfast_in = T.ikstride == 1 || T.pre_op == GO_GATHER;
-  for (int f = threadIdx.x; f < total; f += blockDim.x) {
-    int c, k;
-    if (kfast_in) {
-      c = f / n;
-      k = f - c * n;
-    } else {
-      k = f / cnt;
-      c = f - k * cnt;
+  {
+    const int fast = kfast_in ? n : cnt;  // extent of the fast index
+    const int bq = blockDim.x / fast, br = blockDim.x - bq * fast;
+    int slow = threadIdx.x / fast, fi = threadIdx.x - slow * fast;
+#pragma unroll 4
+    for (int f = threadIdx.x; f < total; f += blockDim.x) {
+      const int c = kfast_in ? slow : fi, k = kfast_in ? fi : slow;
+      sm[c * ld + spad(k)] = tile_load(T, in, c, k);
+      fi += br;
+      slow += bq;
+      if (fi >= fast) {
+        fi -= fast;
+        ++slow;
+      }
     }
-    sm[c * ld + spad(k)] = tile_load(T, in, c, k);
   }
   __syncthreads();
   group_fft_dir(T.dir, sm, cnt, ld, P, T.desc);
   const bool kfast_out = T.okstride == 1 || T.post_op == GO_SCATTER;
-  for (int f = threadIdx.x; f < total; f += blockDim.x) {
-    int c, k;
-    if (kfast_out) {
-      c = f / n;
-      k = f - c * n;
-    } else {
-      k = f / cnt;
-      c = f - k * cnt;
+  {
+    const int fast = kfast_out ? n : cnt;
+    const int bq = blockDim.x / fast, br = blockDim.x - bq * fast;
+    int slow = threadIdx.x / fast, fi = threadIdx.x - slow * fast;
+#pragma unroll 4
+    for (int f = threadIdx.x; f < total; f += blockDim.x) {
+      const int c = kfast_out ? slow : fi, k = kfast_out ? fi : slow;
+      tile_store(T, out, xin, c, k, sm[c * ld + spad(k)], T.dir);
+      fi += br;
+      slow += bq;
+      if (fi >= fast) {
+        fi -= fast;
+        ++slow;
+      }
     }
-    tile_store(T, out, xin, c, k, sm[c * ld + spad(k)], T.dir);
   }
 }
 
