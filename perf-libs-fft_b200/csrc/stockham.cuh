@@ -142,39 +142,66 @@ __device__ __forceinline__ void smem_stage(float2 (&x)[MAXE], float2* sm, int C,
   constexpr int NB = MAXE / R;  // butterflies per thread
   const int nbf = n / R;
   const int total = C * nbf;
-  SFor<0, NB>::run([&](auto bc) {
-    constexpr int b = decltype(bc)::value;
-    const int J = tid + b * nthr;
-    if (J < total) {
-      const int c = J / nbf;
-      const int j = J - c * nbf;
-      const float2* src = sm + c * ld;
+  // butterfly J = tid + b nthr as (transform c, index j), carried across b:
+  // two divisions per stage instead of one per butterfly
+  const int c0 = tid / nbf, j0 = tid - c0 * nbf;
+  const int dq = nthr / nbf, dr = nthr - dq * nbf;
+  {
+    int c = c0, j = j0;
+    SFor<0, NB>::run([&](auto bc) {
+      constexpr int b = decltype(bc)::value;
+      if (tid + b * nthr < total) {
+        const float2* src = sm + c * ld;
 #pragma unroll
-      for (int i = 0; i < R; ++i) x[b * R + i] = src[spad(j + i * nbf)];
-    }
-  });
-  __syncthreads();
-  SFor<0, NB>::run([&](auto bc) {
-    constexpr int b = decltype(bc)::value;
-    const int J = tid + b * nthr;
-    if (J < total) {
-      const int c = J / nbf;
-      const int j = J - c * nbf;
-      const int q = div_ns(j, s);
-      const int r = j - q * s.ns;
-      float2* xb = x + b * R;
-      if (s.ns > 1) {
-        const float2* w = tw + s.tw_off + r;
-#pragma unroll
-        for (int i = 1; i < R; ++i) xb[i] = twmul<DIR>(xb[i], __ldg(w + (i - 1) * s.ns));
+        for (int i = 0; i < R; ++i) x[b * R + i] = src[spad(j + i * nbf)];
       }
-      dft<R, DIR>(xb);
-      float2* dst = sm + c * ld;
-      const int base = q * s.ns * R + r;
+      j += dr;
+      c += dq;
+      if (j >= nbf) {
+        j -= nbf;
+        ++c;
+      }
+    });
+  }
+  __syncthreads();
+  {
+    int c = c0, j = j0;
+    SFor<0, NB>::run([&](auto bc) {
+      constexpr int b = decltype(bc)::value;
+      if (tid + b * nthr < total) {
+        const int q = div_ns(j, s);
+        const int r = j - q * s.ns;
+        float2* xb = x + b * R;
+        if (s.ns > 1) {
+          const float2* w = tw + s.tw_off + r;
+          if constexpr (R >= 16) {
+            // a table entry every fourth factor, products with W^r between
+            const float2 w1 = __ldg(w);
+            float2 wi = w1;
 #pragma unroll
-      for (int i = 0; i < R; ++i) dst[spad(base + i * s.ns)] = xb[i];
-    }
-  });
+            for (int i = 1; i < R; ++i) {
+              if (i > 1) wi = (i & 3) == 1 ? __ldg(w + (i - 1) * s.ns) : cmul(wi, w1);
+              xb[i] = twmul<DIR>(xb[i], wi);
+            }
+          } else {
+#pragma unroll
+            for (int i = 1; i < R; ++i) xb[i] = twmul<DIR>(xb[i], __ldg(w + (i - 1) * s.ns));
+          }
+        }
+        dft<R, DIR>(xb);
+        float2* dst = sm + c * ld;
+        const int base = q * s.ns * R + r;
+#pragma unroll
+        for (int i = 0; i < R; ++i) dst[spad(base + i * s.ns)] = xb[i];
+      }
+      j += dr;
+      c += dq;
+      if (j >= nbf) {
+        j -= nbf;
+        ++c;
+      }
+    });
+  }
   __syncthreads();
 }
 
