@@ -19,6 +19,7 @@
 // PLFFT user would otherwise run (a plan per length, reference
 // src/plfft.cpp:427-517 and the batched plan of src/batched_1d_plan.hpp).
 #include "kernels.h"
+#include "ptx.cuh"
 #include "stockham.cuh"
 
 namespace plfft_b200 {
@@ -43,20 +44,6 @@ __device__ __forceinline__ void group_fft_dir(int dir, float2* sm, int cnt, int 
     group_fft<-1>(sm, cnt, ld, P, desc);
   else
     group_fft<1>(sm, cnt, ld, P, desc);
-}
-
-// prologue: value of element (c, k) of a tile
-__device__ __forceinline__ float2 tile_load(const GTask& T, const float2* in, int c, int k) {
-  const int64_t e = T.ie0 + int64_t(c) * T.iec + int64_t(k) * T.iek;  // logical index
-  switch (T.pre_op) {
-    case GO_GATHER:
-      return in[int64_t(T.perm_in[e]) * T.ikstride];
-    case GO_CHIRP:
-      if (e >= T.pre_len) return make_float2(0.f, 0.f);
-      return cmul(in[int64_t(c) * T.icdist + int64_t(k) * T.ikstride], T.pre_tab[e]);
-    default:
-      return in[int64_t(c) * T.icdist + int64_t(k) * T.ikstride];
-  }
 }
 
 // epilogue: store result element (c, k) of a tile
@@ -108,15 +95,34 @@ __device__ void run_tile(const GTask& T, const GroupPhase& P, float2* sm) {
     const int fast = kfast_in ? n : cnt;  // extent of the fast index
     const int bq = blockDim.x / fast, br = blockDim.x - bq * fast;
     int slow = threadIdx.x / fast, fi = threadIdx.x - slow * fast;
+    // asynchronous copies (all of a thread's loads in flight); the chirp of
+    // a Bluestein prologue is applied in shared memory afterwards
 #pragma unroll 4
     for (int f = threadIdx.x; f < total; f += blockDim.x) {
       const int c = kfast_in ? slow : fi, k = kfast_in ? fi : slow;
-      sm[c * ld + spad(k)] = tile_load(T, in, c, k);
+      float2* dst = sm + c * ld + spad(k);
+      if (T.pre_op == GO_GATHER) {
+        const int64_t e = T.ie0 + int64_t(c) * T.iec + int64_t(k) * T.iek;
+        cp_async8(dst, in + int64_t(T.perm_in[e]) * T.ikstride);
+      } else if (T.pre_op == GO_CHIRP && T.ie0 + int64_t(c) * T.iec + int64_t(k) * T.iek >= T.pre_len) {
+        *dst = make_float2(0.f, 0.f);
+      } else {
+        cp_async8(dst, in + int64_t(c) * T.icdist + int64_t(k) * T.ikstride);
+      }
       fi += br;
       slow += bq;
       if (fi >= fast) {
         fi -= fast;
         ++slow;
+      }
+    }
+    cp_async_wait_all();
+    if (T.pre_op == GO_CHIRP) {
+      __syncthreads();
+      for (int f = threadIdx.x; f < total; f += blockDim.x) {
+        const int c = f / n, k = f - c * n;
+        const int64_t e = T.ie0 + int64_t(c) * T.iec + int64_t(k) * T.iek;
+        if (e < T.pre_len) sm[c * ld + spad(k)] = cmul(sm[c * ld + spad(k)], T.pre_tab[e]);
       }
     }
   }
