@@ -33,7 +33,6 @@ struct qc {
   int re, im;
 };
 
-__device__ __forceinline__ int sat16(int v) { return min(max(v, -32768), 32767); }
 __device__ __forceinline__ int rshr(int v, int s) { return (v + (1 << (s - 1))) >> s; }
 // sqrdmulh by a constant k, |k| <= 32767: never overflows or saturates
 template <int K>
@@ -47,19 +46,19 @@ __device__ __forceinline__ int rdm(int a) {
 // test_q15_codelet_intermediates_never_saturate) shows that only the final
 // output additions can leave int16; intermediate sums, the sqrdmulh constant
 // products and the 32-bit MACs cannot.  Intermediates therefore use plain
-// integer arithmetic (identical results) and only outputs are clamped.
-__device__ __forceinline__ qc qadd(qc a, qc b) { return {sat16(a.re + b.re), sat16(a.im + b.im)}; }
-__device__ __forceinline__ qc qsub(qc a, qc b) { return {sat16(a.re - b.re), sat16(a.im - b.im)}; }
+// integer arithmetic (identical results); outputs saturate when packed.
+// codelet outputs: exact 32-bit sums; the saturation to int16 that sqadd /
+// sqsub apply happens when the output is packed (pack_sat)
+__device__ __forceinline__ qc qadd(qc a, qc b) { return {a.re + b.re, a.im + b.im}; }
+__device__ __forceinline__ qc qsub(qc a, qc b) { return {a.re - b.re, a.im - b.im}; }
 __device__ __forceinline__ qc iadd(qc a, qc b) { return {a.re + b.re, a.im + b.im}; }
 __device__ __forceinline__ qc isub(qc a, qc b) { return {a.re - b.re, a.im - b.im}; }
 // sqrdmulh by -32768 is -a for the |a| < 2^15 that reach it
 __device__ __forceinline__ qc mul_pi(qc z) { return {-z.im, rdm<32767>(z.re)}; }
 __device__ __forceinline__ qc mul_mi(qc z) { return {rdm<32767>(z.im), -z.re}; }
-// 32-bit MAC + rounding shift by 15 of in-range operands (no wrap, no clamp)
-__device__ __forceinline__ int imac2(int a, int ka, int b, int kb) {
-  const int acc = a * ka + b * kb;
-  return (acc >> 15) + ((acc >> 14) & 1);
-}
+// 32-bit MAC + rounding shift by 15 of in-range operands: the accumulators
+// stay far below 2^31 (interval analysis), so adding 2^14 cannot overflow
+__device__ __forceinline__ int imac2(int a, int ka, int b, int kb) { return (a * ka + b * kb + 16384) >> 15; }
 
 constexpr int kC8 = 23170, kC16 = 30273, kS16 = 12539;
 
@@ -176,7 +175,12 @@ constexpr int ilog2_c(int r) { return r <= 1 ? 0 : 1 + ilog2_c(r / 2); }
 
 // int16 pair <-> components (little endian: re in the low half)
 __device__ __forceinline__ qc unpack(int w) { return {(w << 16) >> 16, w >> 16}; }
-__device__ __forceinline__ int pack(qc v) { return (v.re & 0xffff) | (v.im << 16); }
+// saturate both components to int16 and pack (re in the low half)
+__device__ __forceinline__ int pack(qc v) {
+  int d;
+  asm("cvt.pack.sat.s16.s32 %0, %1, %2;" : "=r"(d) : "r"(v.im), "r"(v.re));
+  return d;
+}
 
 // n <= 16: one thread per member
 template <int N, int DIR>
