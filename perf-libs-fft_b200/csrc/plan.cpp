@@ -465,7 +465,7 @@ static std::unique_ptr<Node> make_four_step_pow2(int64_t n, const Layout& lay, i
   node->n2 = n2;
   node->dir = dir;
   node->lay = lay;
-  const int64_t target = int64_t(chunk_mb ? chunk_mb : env_int("PLFFT_B200_FS_CHUNK_MB", 256)) << 20;
+  const int64_t target = int64_t(chunk_mb ? chunk_mb : env_int("PLFFT_B200_FS_CHUNK_MB", 512)) << 20;
   node->chunk = std::max<int64_t>(1, std::min<int64_t>(lay.howmany, target / (n * 8)));
   auto stage_table = [&](int64_t nl, DevBuf& buf) {
     const int e = fourstep_pass_e(int(nl));
@@ -693,7 +693,7 @@ static std::unique_ptr<Node> make_split_bf16(int64_t n, const Layout& lay, int d
                               TwoLevel{nullptr, nullptr, 0, 1}};
     return node;
   }
-  const int64_t target = int64_t(env_int("PLFFT_B200_FS_CHUNK_MB", 256)) << 20;
+  const int64_t target = int64_t(env_int("PLFFT_B200_FS_CHUNK_MB", 512)) << 20;
   node->chunk = std::max<int64_t>(1, std::min<int64_t>(lay.howmany, target / (n * 8)));
   const int64_t L = int64_t(1) << ((ilog2(n) + 1) / 2);
   std::vector<float2> lo(L), hi((n + L - 1) / L);
@@ -803,8 +803,8 @@ std::vector<std::unique_ptr<Node>> make_c2c_candidates(int64_t n, const Layout& 
     if (level >= 2)
       if (auto f = make_four_step_cluster(n, lay, dir, scale)) out.push_back(std::move(f));
     for (int c : {4, 8, 16})
-      for (int mb : {64, 256, 1024}) {
-        if (level < 3 && mb != 256) continue;
+      for (int mb : {128, 512, 1024}) {
+        if (level < 3 && mb != 512) continue;
         if (auto f = make_four_step_pow2(n, lay, dir, scale, c, mb)) out.push_back(std::move(f));
       }
   }
