@@ -130,10 +130,7 @@ int tile_smem_bytes(int ld, int c) { return ld * c * int(sizeof(float2)); }
 
 template <class K>
 static cudaError_t set_smem(K kernel, int bytes) {
-  if (bytes > 32 * 1024) {  // leave room for static shared memory
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  }
-  return cudaSuccess;
+  return ensure_dynamic_smem(reinterpret_cast<const void*>(kernel), bytes);
 }
 
 template <int E, int DIR>

@@ -373,7 +373,7 @@ static cudaError_t run_pow2(const Pow2Launch& L, cudaStream_t st) {
         const int64_t want_groups = L.howmany;
         const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(sm_count(), (want_groups + gp - 1) / gp));
         auto launch = [&](auto kern) {
-          cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+          cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
           if (e != cudaSuccess) return e;
           kern<<<dim3(unsigned(grid)), dim3(gp * T), smem, st>>>(L);
           return cudaGetLastError();
@@ -386,12 +386,8 @@ static cudaError_t run_pow2(const Pow2Launch& L, cudaStream_t st) {
     if (L.slots < 2 || L.slots > kMaxSlots) return cudaErrorInvalidValue;
     auto* k = L.tws ? c2c_pow2_ring_kernel<N, E, DIR, true> : c2c_pow2_ring_kernel<N, E, DIR, false>;
     const int smem = L.slots * pow2_smem_bytes(N, L.g) + (L.tws ? ((L.tw_len + 1) & ~1) * 8 : 0);
-    if (smem > 32 * 1024) {  // leave room for static shared memory
-      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-      if (e != cudaSuccess) return e;
-    }
     int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem);
+    cudaError_t e = cached_blocks_per_sm(reinterpret_cast<const void*>(k), threads, smem, &per_sm);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     // k groups per CTA so that the grid is one resident wave
@@ -402,9 +398,8 @@ static cudaError_t run_pow2(const Pow2Launch& L, cudaStream_t st) {
     return cudaGetLastError();
   }
   const int smem = pow2_smem_bytes(N, L.g);
-  if (smem > 32 * 1024) {  // leave room for static shared memory
-    cudaError_t e = cudaFuncSetAttribute(c2c_pow2_kernel<N, E, DIR>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  {
+    cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(c2c_pow2_kernel<N, E, DIR>), smem);
     if (e != cudaSuccess) return e;
   }
   c2c_pow2_kernel<N, E, DIR><<<dim3(unsigned(ngroups)), dim3(threads), smem, st>>>(L);

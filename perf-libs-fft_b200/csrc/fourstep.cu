@@ -130,9 +130,8 @@ int fourstep_pass_smem(int nl, int c) { return c * ((spad_len(nl) + 1) & ~1) * i
 template <int NL, int E, int DIR>
 static cudaError_t run_fourstep(const FourStepLaunch& L, cudaStream_t st) {
   const int smem = fourstep_pass_smem(NL, L.c);
-  if (smem > 32 * 1024) {  // leave room for static shared memory
-    const cudaError_t e =
-        cudaFuncSetAttribute(fourstep_pass_kernel<NL, E, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  {
+    const cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(fourstep_pass_kernel<NL, E, DIR>), smem);
     if (e != cudaSuccess) return e;
   }
   const int64_t blocks = (L.count + L.c - 1) / L.c;

@@ -133,7 +133,7 @@ int fourstep_cluster_smem() { return 3 * kClCols * ((spad_len(kClNL) + 1) & ~1) 
 cudaError_t launch_fourstep_cluster(int dir, const FourStepClusterLaunch& L, int max_clusters, cudaStream_t st) {
   auto kern = dir < 0 ? fourstep_cluster_kernel<-1> : fourstep_cluster_kernel<1>;
   const int smem = fourstep_cluster_smem();
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
   if (e != cudaSuccess) return e;
   const int64_t ncl = std::max<int64_t>(1, std::min<int64_t>(max_clusters, L.howmany));
   cudaLaunchConfig_t cfg = {};

@@ -112,8 +112,8 @@ cudaError_t launch_fp64_tile(int dir, bool direct, const F64TileLaunch& L, cudaS
   const int smem = direct ? L.desc.n * int(sizeof(double2)) : fp64_tile_smem(L.desc.n);
   auto kern = direct ? (dir < 0 ? fp64_dft_kernel<-1> : fp64_dft_kernel<1>)
                      : (dir < 0 ? fp64_tile_kernel<-1> : fp64_tile_kernel<1>);
-  if (smem > 32 * 1024) {
-    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  {
+    const cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
     if (e != cudaSuccess) return e;
   }
   if (L.ntr <= 0) return cudaSuccess;

@@ -304,6 +304,10 @@ int fp64_tile_smem(int n);
 cudaError_t launch_fp64_tile(int dir, bool direct, const F64TileLaunch& L, cudaStream_t st);
 cudaError_t launch_fp64_real(bool pre, const F64RealLaunch& L, int64_t m0, int64_t cnt, cudaStream_t st);
 
+// launch-time query caches (launch_cache.cpp)
+cudaError_t ensure_dynamic_smem(const void* kernel, int bytes);
+cudaError_t cached_blocks_per_sm(const void* kernel, int threads, int smem, int* blocks);
+
 // kernel entry points (c2c.cu)
 cudaError_t launch_c2c_reg(int e, int dir, const RegLaunch& L, cudaStream_t st);
 cudaError_t launch_c2c_tile(int maxe, int dir, const TileLaunch& L, cudaStream_t st);

@@ -216,11 +216,14 @@ static void build_pipe(const PlanData& p) {
   if (c.howmany < 4 || !p.out_dense || c.istride < 1 || c.ostride < 1) return;
   if (c.idist < (p.nin - 1) * c.istride + 1 || c.odist < (p.nout - 1) * c.ostride + 1) return;
   if (ib + ob < (int64_t(16) << 20)) return;  // too small to gain from overlap
-  // chunks of about 8 MiB of traffic on three streams: the host-to-device
-  // copy of one chunk, the kernels of the previous one and the device-to-host
-  // copy of the one before overlap (measured: 8 MiB chunks on 3 streams beat
-  // 4 MiB chunks on 8 streams, 69 against 60 GB/s end to end for 64 MiB)
-  const int64_t k = std::min<int64_t>(8, std::max<int64_t>(2, (ib + ob) / (int64_t(8) << 20)));
+  // chunks of about 16 MiB of traffic on three streams: the host-to-device
+  // copy of one chunk, the kernels of another and the device-to-host copy
+  // of a third overlap (measured for 64 MiB: 2 / 4 / 8 / 16 / 32 MiB chunks
+  // gave 56 / 61 / 67 / 72 / 67 GB/s end to end; concurrent pinned copies
+  // alone reach 95 GB/s)
+  int64_t chunk_mb = 16;
+  if (const char* v = std::getenv("PLFFT_B200_PIPE_MB")) chunk_mb = std::max(1, std::atoi(v));
+  const int64_t k = std::min<int64_t>(64, std::max<int64_t>(2, (ib + ob) / (chunk_mb << 20)));
   const int64_t per = (c.howmany + k - 1) / k;
   const int64_t tail = c.howmany - (c.howmany - 1) / per * per;
   std::string why, note;

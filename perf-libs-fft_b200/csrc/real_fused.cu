@@ -182,9 +182,8 @@ static cudaError_t run_real_fused(const RealFusedLaunch& L, cudaStream_t st) {
   constexpr int T = M / E;
   constexpr int PITCH = (spad_len_c(M) + 1) & ~1;
   const int smem = L.g * PITCH * int(sizeof(float2));
-  if (smem > 32 * 1024) {  // leave room for static shared memory
-    const cudaError_t e =
-        cudaFuncSetAttribute(real_fused_kernel<M, E, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  {
+    const cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(real_fused_kernel<M, E, KIND>), smem);
     if (e != cudaSuccess) return e;
   }
   const int64_t blocks = (L.howmany + L.g - 1) / L.g;

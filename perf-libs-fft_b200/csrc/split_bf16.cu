@@ -231,9 +231,8 @@ template <int NL, int DIR>
 static cudaError_t run_sb(const FourStepLaunch& L, const uint32_t* dftm, cudaStream_t st) {
   constexpr int C = kSbTile / NL;
   const int smem = C * ((spad_len(NL) + 1) & ~1) * int(sizeof(float2));
-  if (smem > 32 * 1024) {
-    const cudaError_t e =
-        cudaFuncSetAttribute(split_bf16_pass_kernel<NL, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  {
+    const cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(split_bf16_pass_kernel<NL, DIR>), smem);
     if (e != cudaSuccess) return e;
   }
   const int64_t blocks = (L.count + C - 1) / C;
