@@ -31,20 +31,22 @@ namespace plfft_b200 {
 constexpr int kSbThreads = 256;
 constexpr int kSbTile = 4096;  // complex elements per CTA tile
 
-__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo, __nv_bfloat16 hi) {
-  return uint32_t(__bfloat16_as_ushort(lo)) | (uint32_t(__bfloat16_as_ushort(hi)) << 16);
-}
 
-// three-term split of a pair of floats into packed bf16x2 words
+// three-term split of a pair of floats into packed bf16x2 words by
+// truncation: the high 16 bits of a float are a bf16 value, so
+// x0 = hi16(x), r = x - x0 (exact), x1 = hi16(r), r2 = r - x1 (exact),
+// x2 = hi16(r2); the three 8-bit significands carry 24 bits of x, and
+// __byte_perm gathers the high halves of two floats into one word
+__device__ __forceinline__ float hi16(float x) { return __uint_as_float(__float_as_uint(x) & 0xffff0000u); }
+__device__ __forceinline__ uint32_t pack_hi(float lo, float hi) {
+  return __byte_perm(__float_as_uint(lo), __float_as_uint(hi), 0x7632);
+}
 __device__ __forceinline__ void split3(float a, float b, uint32_t& w0, uint32_t& w1, uint32_t& w2) {
-  const __nv_bfloat16 a0 = __float2bfloat16_rn(a), b0 = __float2bfloat16_rn(b);
-  const float ra = a - __bfloat162float(a0), rb = b - __bfloat162float(b0);
-  const __nv_bfloat16 a1 = __float2bfloat16_rn(ra), b1 = __float2bfloat16_rn(rb);
-  const __nv_bfloat16 a2 = __float2bfloat16_rn(ra - __bfloat162float(a1));
-  const __nv_bfloat16 b2 = __float2bfloat16_rn(rb - __bfloat162float(b1));
-  w0 = pack_bf16(a0, b0);
-  w1 = pack_bf16(a1, b1);
-  w2 = pack_bf16(a2, b2);
+  const float ra = a - hi16(a), rb = b - hi16(b);
+  const float r2a = ra - hi16(ra), r2b = rb - hi16(rb);
+  w0 = pack_hi(a, b);
+  w1 = pack_hi(ra, rb);
+  w2 = pack_hi(r2a, r2b);
 }
 
 // D += A (16x16 bf16, row) * B (16x8 bf16, col), FP32 accumulate (no side
@@ -153,7 +155,7 @@ __device__ __forceinline__ void sb_stage(float2* tile, int pitch, int ns, const 
 }
 
 template <int NL, int DIR>
-__global__ void __launch_bounds__(kSbThreads) split_bf16_pass_kernel(const FourStepLaunch L,
+__global__ void __launch_bounds__(kSbThreads, 2) split_bf16_pass_kernel(const FourStepLaunch L,
                                                                      const uint32_t* __restrict__ dftm) {
   constexpr int C = kSbTile / NL;  // sub-transforms per CTA
   constexpr int S = NL == 256 ? 2 : 3;
