@@ -7,19 +7,19 @@ Default workload (the configuration the headline metric is quoted on):
 plain C2C FP32 forward, N=1024, batch=4096, unit stride, contiguous,
 out-of-place, no scaling; re/im i.i.d. U[-1,1) from a seed.  Other workloads
 (--workload) cover the remaining configurations: R2C/C2R round trip, DCT-II,
-DST-II, Q0.15, the long C2C lengths, the grouped mixed-length batch and the
-differentiation step.
+DST-II, Q0.15, the long C2C lengths in plain FP32 and split-BF16 precision,
+the grouped mixed-length batch and the differentiation step.
 
 One JSON line on rank 0.  `value` = algorithmic GB/s (one read of every input
-plus one write of every output per step, BASELINE.md definitions) summed over
-ranks, device-timed with CUDA events on the launching stream, max over ranks.
+plus one write of every output per step) summed over ranks, device-timed
+with CUDA events on the launching stream, max over ranks.
 Inputs rotate over buffer sets totalling more than 4x the 126 MB L2, so no
 step starts L2-warm.  `e2e` is the same metric through the public entry point
 with pinned host buffers (host->device and device->host copies inside the
 timed region).  `--impl reference` times the CPU implementation of the path:
 the FP64 port of the reference's transform definitions in oracle/ (the
-reference itself is AArch64-only and does not build on this x86_64 host),
-on all host cores, on a bounded sample of the same workload.
+reference itself is AArch64-only and does not build on an x86_64 host), on
+all host cores, as K steps of a calibrated sample of the same workload.
 
 Multi-GPU (torchrun, one rank per GPU): every rank runs the full workload on
 its own GPU (batch replicas, weak scaling); there is no data-path collective.
