@@ -201,6 +201,8 @@ struct RealFusedLaunch {
   const float2* rot;   // exp(-i pi k / 2N), k = 0..M
   int pairs_in, pairs_out;  // real data may be moved as aligned float pairs
   int e;                    // elements per thread of the length-M FFT
+  int wmode;                // adjoint weights: 1 C2R input bins 0<k<M times 1/2,
+                            // 2 R2C output bins 0<k<M times 2
 };
 bool real_fused_supported(int m);
 int real_fused_e(int m);

@@ -154,7 +154,8 @@ std::unique_ptr<Node> make_realwrap_node(int kind, int64_t n, const Layout& lay,
 
 // One-kernel R2C / C2R / DCT-II / DST-II (FusedRealKind) for N = 2M, M a
 // power of two in [64, 8192], unit strides; nullptr when not applicable.
-std::unique_ptr<Node> make_real_fused_node(int kind, int64_t n, const Layout& lay, float scale);
+// wmode: adjoint weights (RealFusedLaunch::wmode), 0 for the plain transform.
+std::unique_ptr<Node> make_real_fused_node(int kind, int64_t n, const Layout& lay, float scale, int wmode = 0);
 
 // Adjoint of a plan's transform (same scale, input/output layouts swapped):
 // the conjugate-direction C2C, or the transposed real transform expressed

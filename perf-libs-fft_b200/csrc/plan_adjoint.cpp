@@ -30,9 +30,11 @@ std::unique_ptr<Node> make_adjoint_node(const ConfigData& c, std::string* why) {
   switch (c.kind) {
     case TKind::C2C:
       return make_c2c_node(c.n, lay, -c.payload, scale, c.precision, why);
-    case TKind::R2C:
+    case TKind::R2C:  // one fused kernel where it applies
+      if (auto f = make_real_fused_node(FR_C2R, c.n, lay, scale, 1)) return f;
       return make_realwrap_node(RW_C2R, c.n, lay, scale, why, AW_HERM_HALF, AW_NONE);
     case TKind::C2R:
+      if (auto f = make_real_fused_node(FR_R2C, c.n, lay, scale, 2)) return f;
       return make_realwrap_node(RW_R2C, c.n, lay, scale, why, AW_NONE, AW_HERM_DOUBLE);
     case TKind::R2R:
       switch (c.payload) {

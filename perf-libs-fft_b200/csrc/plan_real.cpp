@@ -140,7 +140,7 @@ struct RealFusedNode : Node {
 
 }  // namespace
 
-std::unique_ptr<Node> make_real_fused_node(int kind, int64_t n, const Layout& lay, float scale) {
+std::unique_ptr<Node> make_real_fused_node(int kind, int64_t n, const Layout& lay, float scale, int wmode) {
   if (n % 2 || !real_fused_supported(int(n / 2)) || lay.istride != 1 || lay.ostride != 1) return nullptr;
   if (std::getenv("PLFFT_B200_NO_FUSED_REAL")) return nullptr;
   const int m = int(n / 2);
@@ -180,6 +180,7 @@ std::unique_ptr<Node> make_real_fused_node(int kind, int64_t n, const Layout& la
   node->base.g = std::max(1, 128 / t);
   if (const char* v = std::getenv("PLFFT_B200_RF_G")) node->base.g = std::max(1, std::atoi(v));
   node->base.e = e;
+  node->base.wmode = wmode;
   node->base.scale = scale;
   node->base.tw = node->tab.as<float2>();
   node->base.post = node->tab.as<float2>() + post_off;

@@ -65,7 +65,8 @@ __device__ __forceinline__ void finish_real(float2 (&v)[E], const RealFusedLaunc
     auto out_k = [&](int k) {
       const float2 V = real_split(mine, k, M, L.post);
       if constexpr (KIND == FR_R2C) {
-        static_cast<float2*>(L.out)[b * L.odist + k] = cscale(V, s);
+        const float sk = (L.wmode == 2 && k > 0 && k < M) ? 2.f * s : s;
+        static_cast<float2*>(L.out)[b * L.odist + k] = cscale(V, sk);
       } else {
         const float2 c = cmul(__ldg(L.rot + k), V);
         float* y = static_cast<float*>(L.out) + b * L.odist;
@@ -132,6 +133,9 @@ __global__ void __launch_bounds__(pow2_max_threads<E>()) real_fused_kernel(const
       if (k == 0) {
         xk.y = 0.f;
         xm.y = 0.f;
+      } else if (L.wmode == 1) {  // bins 0 < k < M (both k and M - k here)
+        xk = cscale(xk, 0.5f);
+        xm = cscale(xm, 0.5f);
       }
       const float2 cm = make_float2(xm.x, -xm.y);
       const float2 a = cadd(xk, cm);
