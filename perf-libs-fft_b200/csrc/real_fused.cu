@@ -122,6 +122,7 @@ __global__ void __launch_bounds__(pow2_max_threads<E>()) real_fused_kernel(const
     }
   } else if constexpr (KIND == FR_C2R) {
     const float2* X = static_cast<const float2*>(L.in) + (live ? b * L.idist : 0);
+    const float hw = L.wmode == 1 ? 0.5f : 1.f;
 #pragma unroll
     for (int q = 0; q < E; ++q) {
       const int k = t + T * q;
@@ -130,13 +131,13 @@ __global__ void __launch_bounds__(pow2_max_threads<E>()) real_fused_kernel(const
         continue;
       }
       float2 xk = X[k], xm = X[M - k];
-      if (k == 0) {
-        xk.y = 0.f;
-        xm.y = 0.f;
-      } else if (L.wmode == 1) {  // bins 0 < k < M (both k and M - k here)
-        xk = cscale(xk, 0.5f);
-        xm = cscale(xm, 0.5f);
-      }
+      // k = 0: imaginary parts of X_0 and X_M ignored; adjoint weights halve
+      // bins 0 < k < M (both k and M - k here); selects, not branches, so
+      // the loads of every q stay in flight together
+      const bool k0 = k == 0;
+      const float w = k0 ? 1.f : hw;
+      xk = make_float2(xk.x * w, k0 ? 0.f : xk.y * w);
+      xm = make_float2(xm.x * w, k0 ? 0.f : xm.y * w);
       const float2 cm = make_float2(xm.x, -xm.y);
       const float2 a = cadd(xk, cm);
       const float2 d = csub(xk, cm);
