@@ -51,6 +51,7 @@ class Workload:
     name = ""
     desc = ""
     dtype = "f32"
+    data = "synthetic (seeded U[-1,1) re/im)"
     profile = None  # profiles/<name>.md holding traffic_bytes_per_launch
 
     def config(self):
@@ -70,6 +71,8 @@ class PlanWorkload(Workload):
 
     def __init__(self, name, desc, kind, n, batch, r2r=None, precision=0, profile=None):
         self.name, self.desc, self.kind, self.n, self.batch = name, desc, kind, n, batch
+        if kind != "c2c":
+            self.data = "synthetic (seeded real U[-1,1))"
         self.r2r, self.precision, self.profile = r2r, precision, profile
 
     def sizes(self):
@@ -359,6 +362,7 @@ class Q15Workload(PlanWorkload):
     """Q0.15 fixed-point C2C (int16 re/im pairs, scaled by 1/N)."""
 
     dtype = "int16"
+    data = "synthetic (seeded int16 re/im uniform in [-2^14, 2^14))"
 
     def __init__(self, name, desc, n, batch):
         super().__init__(name, desc, "c2c", n, batch, profile="q15_two_stage_n256_b16384")
@@ -597,7 +601,7 @@ def main():
                 "impl": "reference", "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
                 "ms_per_step": ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64" if w.dtype == "f32" else w.dtype,
-                "data": "synthetic (seeded U[-1,1))", "config": w.config(), "cpu_baseline": cpu,
+                "data": w.data, "config": w.config(), "cpu_baseline": cpu,
                 "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -694,7 +698,7 @@ def main():
             "metric": f"{w.name} GB/s (algorithmic bytes)", "value": value, "unit": "GB/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": w.dtype,
-            "data": "synthetic (seeded U[-1,1) re/im)",
+            "data": w.data,
             "config": dict(w.config(), l2="inputs rotate over buffer sets totalling > 4x L2",
                            parallelism=f"batch replicas x{world}, no collective"),
             "gflops": w.flops() * world / (ms_per_step * 1e-3) / 1e9,
