@@ -189,7 +189,7 @@ int group_max_smem_elems();
 
 // Fused single-kernel real transforms for N = 2M, M a power of two
 // (real_fused.cu).  Distances count elements of each buffer's own type.
-enum FusedRealKind { FR_R2C = 0, FR_C2R = 1, FR_DCT2 = 2, FR_DST2 = 3 };
+enum FusedRealKind { FR_R2C = 0, FR_C2R = 1, FR_DCT2 = 2, FR_DST2 = 3, FR_DCT3 = 4, FR_DST3 = 5 };
 struct RealFusedLaunch {
   const void* in;
   void* out;
@@ -202,7 +202,8 @@ struct RealFusedLaunch {
   int pairs_in, pairs_out;  // real data may be moved as aligned float pairs
   int e;                    // elements per thread of the length-M FFT
   int wmode;                // adjoint weights: 1 C2R input bins 0<k<M times 1/2,
-                            // 2 R2C output bins 0<k<M times 2
+                            // 2 R2C output bins 0<k<M times 2, 3 DCT-III input
+                            // element 0 (DST-III: element N-1) times 2
 };
 bool real_fused_supported(int m);
 int real_fused_e(int m);

@@ -65,6 +65,8 @@ static std::unique_ptr<Node> make_root(const ConfigData& c, const Layout& lay, b
                                   RW_DST3, RW_DST4, RW_DHT,  RW_R2HC, RW_HC2R};
         if (c.payload == PLFFT_R2R_DCT_2) root = make_real_fused_node(FR_DCT2, c.n, lay, scale);
         if (c.payload == PLFFT_R2R_DST_2) root = make_real_fused_node(FR_DST2, c.n, lay, scale);
+        if (c.payload == PLFFT_R2R_DCT_3) root = make_real_fused_node(FR_DCT3, c.n, lay, scale);
+        if (c.payload == PLFFT_R2R_DST_3) root = make_real_fused_node(FR_DST3, c.n, lay, scale);
         if (!root) root = make_realwrap_node(map[c.payload], c.n, lay, scale, why);
         break;
       }

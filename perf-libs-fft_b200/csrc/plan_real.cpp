@@ -130,7 +130,7 @@ struct RealFusedNode : Node {
     return launch_real_fused(kind, m, L, st);
   }
   std::string describe() const override {
-    static const char* names[] = {"r2c", "c2r", "dct2", "dst2"};
+    static const char* names[] = {"r2c", "c2r", "dct2", "dst2", "dct3", "dst3"};
     std::ostringstream o;
     o << "(" << names[kind] << "-fused n=" << 2 * m << " m=" << m << " e=" << base.e << " g=" << base.g
       << ")";

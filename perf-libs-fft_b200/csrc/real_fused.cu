@@ -12,6 +12,11 @@
 //        V = DFT_N(v) by the R2C route above, then
 //        y_k = 2 Re(e^{-i pi k/2N} V_k), y_{N-k} = -2 Im(e^{-i pi k/2N} V_k).
 // DST-II: DST-II(x)_k = DCT-II((-1)^j x_j)_{N-1-k}.
+// DCT-III (the transpose of DCT-II): with y_N = 0,
+//        W_k = e^{i pi k/2N} (y_k - i y_{N-k}), k = 0..M, is a Hermitian half
+//        spectrum; u = its length-N backward real DFT (the C2R route above);
+//        x_{2j} = u_j, x_{2j+1} = u_{N-1-j} (Makhoul's permutation undone).
+// DST-III: DST-III(y)_j = (-1)^j DCT-III(y_{N-1-k})_j.
 // These are the reference's R2C / C2R twiddle levels
 // (src/level_ab_t_r2c.cpp:17-120, src/level_ab_t_c2r.cpp:17-99) and its
 // DCT-II / DST-II pre/post passes (src/r2r_buffer_helper.hpp:316-335,
@@ -40,7 +45,22 @@ __device__ __forceinline__ void finish_real(float2 (&v)[E], const RealFusedLaunc
   constexpr int T = P::T;
   constexpr int N = 2 * M;
   const float s = L.scale;
-  if constexpr (KIND == FR_C2R) {
+  if constexpr (KIND == FR_DCT3 || KIND == FR_DST3) {
+    // u_{2m} = Re z_m, u_{2m+1} = Im z_m staged as N floats, then written in
+    // x order: x_{2j} = u_j, x_{2j+1} = u_{N-1-j}
+    float* us = reinterpret_cast<float*>(mine);
+    sync();  // last exchange fully read
+#pragma unroll
+    for (int q = 0; q < E; ++q) reinterpret_cast<float2*>(us)[t + T * q] = v[q];
+    sync();
+    if (!live) return;
+    float* x = static_cast<float*>(L.out) + b * L.odist;
+#pragma unroll
+    for (int f = t; f < N; f += T) {
+      const float u = (f & 1) ? us[N - 1 - (f >> 1)] : us[f >> 1];
+      x[f] = (KIND == FR_DST3 && (f & 1)) ? -u * s : u * s;
+    }
+  } else if constexpr (KIND == FR_C2R) {
     if (!live) return;
     float* x = static_cast<float*>(L.out) + b * L.odist;
 #pragma unroll
@@ -92,7 +112,7 @@ __global__ void __launch_bounds__(pow2_max_threads<E>()) real_fused_kernel(const
   constexpr int T = P::T;
   constexpr int N = 2 * M;
   constexpr int PITCH = (spad_len_c(M) + 1) & ~1;
-  constexpr int DIR = KIND == FR_C2R ? 1 : -1;
+  constexpr int DIR = (KIND == FR_C2R || KIND == FR_DCT3 || KIND == FR_DST3) ? 1 : -1;
   extern __shared__ __align__(128) unsigned char smraw[];
   const int G = L.g;
   const int grp = threadIdx.x / T;
@@ -119,6 +139,30 @@ __global__ void __launch_bounds__(pow2_max_threads<E>()) real_fused_kernel(const
         v[q] = reinterpret_cast<const float2*>(x)[m];
       else
         v[q] = make_float2(x[2 * m], x[2 * m + 1]);
+    }
+  } else if constexpr (KIND == FR_DCT3 || KIND == FR_DST3) {
+    const float* y = static_cast<const float*>(L.in) + (live ? b * L.idist : 0);
+    const float w0 = L.wmode == 3 ? 2.f : 1.f;
+    // y_j of the (DST-III: reversed) input, y_N = 0
+    auto Y = [&](int j) {
+      if (!live || j >= N) return 0.f;
+      const float val = KIND == FR_DST3 ? y[N - 1 - j] : y[j];
+      return j == 0 ? w0 * val : val;
+    };
+    // W_k = conj(rot_k) (y_k - i y_{N-k})
+    auto Wk = [&](int k) { return cmulc(make_float2(Y(k), -Y(N - k)), __ldg(L.rot + k)); };
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+      const int k = t + T * q;
+      float2 xk = Wk(k), xm = Wk(M - k);
+      const bool k0 = k == 0;  // imaginary parts of W_0 and W_M ignored
+      xk.y = k0 ? 0.f : xk.y;
+      xm.y = k0 ? 0.f : xm.y;
+      const float2 cm = make_float2(xm.x, -xm.y);
+      const float2 a = cadd(xk, cm);
+      const float2 d = csub(xk, cm);
+      const float2 wd = cmulc(d, __ldg(L.post + k));  // conj(W_N^k) * d
+      v[q] = cadd(a, make_float2(-wd.y, wd.x));       // a + i * wd
     }
   } else if constexpr (KIND == FR_C2R) {
     const float2* X = static_cast<const float2*>(L.in) + (live ? b * L.idist : 0);
@@ -203,6 +247,8 @@ static cudaError_t run_real_fused_kind(int kind, const RealFusedLaunch& L, cudaS
     case FR_C2R: return run_real_fused<M, E, FR_C2R>(L, st);
     case FR_DCT2: return run_real_fused<M, E, FR_DCT2>(L, st);
     case FR_DST2: return run_real_fused<M, E, FR_DST2>(L, st);
+    case FR_DCT3: return run_real_fused<M, E, FR_DCT3>(L, st);
+    case FR_DST3: return run_real_fused<M, E, FR_DST3>(L, st);
   }
   return cudaErrorInvalidValue;
 }
