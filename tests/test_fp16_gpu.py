@@ -80,3 +80,19 @@ def test_fp16_dct2_in_place_and_host():
     plan.execute(buf.ctypes.data, buf.ctypes.data)  # host pointers, in place
     ref = oracle.r2r(x.astype(np.float64), "DCT_2")
     assert oracle.rel_l2(buf.astype(np.float64), ref) <= TOL
+
+
+def test_fp16_c2c_in_place():
+    import plfft
+    import torch
+
+    n, hm = 4096, 8
+    rng = np.random.default_rng(11)
+    xh = np.stack([rng.uniform(-1, 1, (hm, n)), rng.uniform(-1, 1, (hm, n))], -1).astype(np.float16)
+    plan = plfft.make_plan("c2c", n, hm, direction=-1, data_type=plfft.DataType.FP16,
+                           alias=plfft.IoAlias.MAY_ALIAS)
+    d = _dev(xh)
+    plan.execute(d.data_ptr(), d.data_ptr())
+    y = _host(d, np.float16, (hm, n, 2)).astype(np.float64)
+    ref = oracle.c2c(xh[..., 0].astype(np.float64) + 1j * xh[..., 1].astype(np.float64), -1, method="fft")
+    assert oracle.rel_l2(y[..., 0] + 1j * y[..., 1], ref) <= TOL

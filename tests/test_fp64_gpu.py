@@ -71,3 +71,18 @@ def test_fp64_r2r_fails_plan_creation():
     with pytest.raises(plfft.PlfftError) as e:
         plfft.make_plan("r2r", 64, 1, r2r_kind=plfft.R2RKind.DCT_2, data_type=plfft.DataType.FP64)
     assert e.value.status == plfft.Status.PLAN_CREATION_FAILED
+
+
+@pytest.mark.parametrize("n", [1024, 3 * 4096, 97])
+def test_fp64_c2c_in_place_host(n):
+    """In place on host buffers (staged through the device)."""
+    import plfft
+
+    rng = np.random.default_rng(n + 7)
+    hm = 3
+    x = rng.uniform(-1, 1, (hm, n)) + 1j * rng.uniform(-1, 1, (hm, n))
+    buf = x.copy()
+    plan = plfft.make_plan("c2c", n, hm, direction=1, data_type=plfft.DataType.FP64,
+                           alias=plfft.IoAlias.MAY_ALIAS)
+    plan.execute(buf.ctypes.data, buf.ctypes.data)
+    assert oracle.rel_l2(buf, oracle.c2c(x, 1, method="fft")) <= tol64(n)

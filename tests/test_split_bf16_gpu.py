@@ -63,3 +63,18 @@ def test_split_bf16_unsupported_lengths_fail():
         with pytest.raises(plfft.PlfftError) as e:
             plfft.make_plan("c2c", n, 2, precision=plfft.Precision.SPLIT_BF16)
         assert e.value.status == plfft.Status.PLAN_CREATION_FAILED
+
+
+@pytest.mark.parametrize("n", [4096, 65536])
+def test_split_bf16_in_place_host(n):
+    """In place on host buffers: the plan stages through the device."""
+    import plfft
+
+    rng = np.random.default_rng(n)
+    hm = 2
+    x = (rng.uniform(-1, 1, (hm, n)) + 1j * rng.uniform(-1, 1, (hm, n))).astype(np.complex64)
+    buf = x.copy()
+    plan = plfft.make_plan("c2c", n, hm, direction=-1, precision=plfft.Precision.SPLIT_BF16,
+                           alias=plfft.IoAlias.MAY_ALIAS)
+    plan.execute(buf.ctypes.data, buf.ctypes.data)
+    assert oracle.rel_l2(buf, oracle.c2c(x.astype(np.complex128), -1, method="fft")) <= 1e-6
