@@ -189,7 +189,7 @@ int group_max_smem_elems();
 
 // Fused single-kernel real transforms for N = 2M, M a power of two
 // (real_fused.cu).  Distances count elements of each buffer's own type.
-enum FusedRealKind { FR_R2C = 0, FR_C2R = 1, FR_DCT2 = 2, FR_DST2 = 3, FR_DCT3 = 4, FR_DST3 = 5 };
+enum FusedRealKind { FR_R2C = 0, FR_C2R = 1, FR_DCT2 = 2, FR_DST2 = 3, FR_DCT3 = 4, FR_DST3 = 5, FR_DCT4 = 6, FR_DST4 = 7 };
 struct RealFusedLaunch {
   const void* in;
   void* out;
@@ -197,8 +197,8 @@ struct RealFusedLaunch {
   int g;  // transforms per CTA
   float scale;
   const float2* tw;    // stage twiddles of the length-M complex FFT
-  const float2* post;  // W_N^k, k = 0..M
-  const float2* rot;   // exp(-i pi k / 2N), k = 0..M
+  const float2* post;  // W_N^k, k = 0..M (DCT-IV / DST-IV: exp(i pi p / N), p < M)
+  const float2* rot;   // exp(-i pi k / 2N), k = 0..M (DCT-IV / DST-IV: exp(i pi (4q+1) / 4N), q < M)
   int pairs_in, pairs_out;  // real data may be moved as aligned float pairs
   int e;                    // elements per thread of the length-M FFT
   int wmode;                // adjoint weights: 1 C2R input bins 0<k<M times 1/2,

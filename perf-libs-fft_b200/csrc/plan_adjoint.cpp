@@ -43,13 +43,17 @@ std::unique_ptr<Node> make_adjoint_node(const ConfigData& c, std::string* why) {
           if (auto f = make_real_fused_node(FR_DCT3, c.n, lay, scale, 3)) return f;
           return make_realwrap_node(RW_DCT3, c.n, lay, scale, why, AW_FIRST_X2, AW_NONE);
         case PLFFT_R2R_DCT_3: return make_realwrap_node(RW_DCT2, c.n, lay, scale, why, AW_NONE, AW_FIRST_HALF);
-        case PLFFT_R2R_DCT_4: return make_realwrap_node(RW_DCT4, c.n, lay, scale, why);
+        case PLFFT_R2R_DCT_4:  // self-adjoint
+          if (auto f = make_real_fused_node(FR_DCT4, c.n, lay, scale)) return f;
+          return make_realwrap_node(RW_DCT4, c.n, lay, scale, why);
         case PLFFT_R2R_DST_1: return make_realwrap_node(RW_DST1, c.n, lay, scale, why);
         case PLFFT_R2R_DST_2:
           if (auto f = make_real_fused_node(FR_DST3, c.n, lay, scale, 3)) return f;
           return make_realwrap_node(RW_DST3, c.n, lay, scale, why, AW_LAST_X2, AW_NONE);
         case PLFFT_R2R_DST_3: return make_realwrap_node(RW_DST2, c.n, lay, scale, why, AW_NONE, AW_LAST_HALF);
-        case PLFFT_R2R_DST_4: return make_realwrap_node(RW_DST4, c.n, lay, scale, why);
+        case PLFFT_R2R_DST_4:
+          if (auto f = make_real_fused_node(FR_DST4, c.n, lay, scale)) return f;
+          return make_realwrap_node(RW_DST4, c.n, lay, scale, why);
         case PLFFT_R2R_DHT: return make_realwrap_node(RW_DHT, c.n, lay, scale, why);
         case PLFFT_R2R_R2HC: return make_realwrap_node(RW_HC2R, c.n, lay, scale, why, AW_HC_HALF, AW_NONE);
         case PLFFT_R2R_HC2R: return make_realwrap_node(RW_R2HC, c.n, lay, scale, why, AW_NONE, AW_HC_DOUBLE);

@@ -130,7 +130,7 @@ struct RealFusedNode : Node {
     return launch_real_fused(kind, m, L, st);
   }
   std::string describe() const override {
-    static const char* names[] = {"r2c", "c2r", "dct2", "dst2", "dct3", "dst3"};
+    static const char* names[] = {"r2c", "c2r", "dct2", "dst2", "dct3", "dst3", "dct4", "dst4"};
     std::ostringstream o;
     o << "(" << names[kind] << "-fused n=" << 2 * m << " m=" << m << " e=" << base.e << " g=" << base.g
       << ")";
@@ -157,17 +157,18 @@ std::unique_ptr<Node> make_real_fused_node(int kind, int64_t n, const Layout& la
   for (int i = 0; i < ke; ++i) radices.push_back(e);
   std::vector<float2> tw;
   make_desc(m, radices, tw);
+  const bool iv = kind == FR_DCT4 || kind == FR_DST4;
   const size_t post_off = tw.size();
-  for (int k = 0; k <= m; ++k) {  // W_N^k
+  for (int k = 0; k <= m; ++k) {  // W_N^k; DCT-IV / DST-IV: exp(i pi k / N) = W_{2N}^{-k}
     double c, s;
-    unit_root(k, n, c, s);
-    tw.push_back(make_float2(float(c), float(-s)));
+    unit_root(iv ? 2 * int64_t(k) : k, iv ? 4 * n : n, c, s);
+    tw.push_back(make_float2(float(c), float(iv ? s : -s)));
   }
   const size_t rot_off = tw.size();
-  for (int k = 0; k <= m; ++k) {  // exp(-i pi k / 2N) = W_{4N}^k
+  for (int k = 0; k <= m; ++k) {  // exp(-i pi k / 2N) = W_{4N}^k; DCT-IV / DST-IV: exp(i pi (4k+1) / 4N)
     double c, s;
-    unit_root(k, 4 * n, c, s);
-    tw.push_back(make_float2(float(c), float(-s)));
+    unit_root(iv ? 4 * int64_t(k) + 1 : k, iv ? 8 * n : 4 * n, c, s);
+    tw.push_back(make_float2(float(c), float(iv ? s : -s)));
   }
   auto node = std::make_unique<RealFusedNode>();
   node->kind = kind;

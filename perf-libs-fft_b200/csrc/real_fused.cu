@@ -17,6 +17,9 @@
 //        spectrum; u = its length-N backward real DFT (the C2R route above);
 //        x_{2j} = u_j, x_{2j+1} = u_{N-1-j} (Makhoul's permutation undone).
 // DST-III: DST-III(y)_j = (-1)^j DCT-III(y_{N-1-k})_j.
+// DCT-IV: c_p = (x_{2p} - i x_{N-1-2p}) e^{i pi p/N}, C = backward DFT_M(c),
+//        S_q = e^{i pi (q + 1/4)/N} C_q: y_{2q} = 2 Re S_q, y_{N-1-2q} =
+//        2 Im S_q.  DST-IV(x)_k = (-1)^k DCT-IV(x_{N-1-n})_k.
 // These are the reference's R2C / C2R twiddle levels
 // (src/level_ab_t_r2c.cpp:17-120, src/level_ab_t_c2r.cpp:17-99) and its
 // DCT-II / DST-II pre/post passes (src/r2r_buffer_helper.hpp:316-335,
@@ -45,7 +48,23 @@ __device__ __forceinline__ void finish_real(float2 (&v)[E], const RealFusedLaunc
   constexpr int T = P::T;
   constexpr int N = 2 * M;
   const float s = L.scale;
-  if constexpr (KIND == FR_DCT3 || KIND == FR_DST3) {
+  if constexpr (KIND == FR_DCT4 || KIND == FR_DST4) {
+    // S_q = rot_q C_q, staged as y_{2q} = 2 Re S_q, y_{N-1-2q} = +-2 Im S_q
+    float* us = reinterpret_cast<float*>(mine);
+    sync();  // last exchange fully read
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+      const int m = t + T * q;
+      const float2 S = cmul(__ldg(L.rot + m), v[q]);
+      us[2 * m] = 2.f * S.x;
+      us[N - 1 - 2 * m] = KIND == FR_DST4 ? -2.f * S.y : 2.f * S.y;
+    }
+    sync();
+    if (!live) return;
+    float* x = static_cast<float*>(L.out) + b * L.odist;
+#pragma unroll
+    for (int f = t; f < N; f += T) x[f] = us[f] * s;
+  } else if constexpr (KIND == FR_DCT3 || KIND == FR_DST3) {
     // u_{2m} = Re z_m, u_{2m+1} = Im z_m staged as N floats, then written in
     // x order: x_{2j} = u_j, x_{2j+1} = u_{N-1-j}
     float* us = reinterpret_cast<float*>(mine);
@@ -112,7 +131,7 @@ __global__ void __launch_bounds__(pow2_max_threads<E>()) real_fused_kernel(const
   constexpr int T = P::T;
   constexpr int N = 2 * M;
   constexpr int PITCH = (spad_len_c(M) + 1) & ~1;
-  constexpr int DIR = (KIND == FR_C2R || KIND == FR_DCT3 || KIND == FR_DST3) ? 1 : -1;
+  constexpr int DIR = (KIND == FR_C2R || KIND == FR_DCT3 || KIND == FR_DST3 || KIND == FR_DCT4 || KIND == FR_DST4) ? 1 : -1;
   extern __shared__ __align__(128) unsigned char smraw[];
   const int G = L.g;
   const int grp = threadIdx.x / T;
@@ -139,6 +158,15 @@ __global__ void __launch_bounds__(pow2_max_threads<E>()) real_fused_kernel(const
         v[q] = reinterpret_cast<const float2*>(x)[m];
       else
         v[q] = make_float2(x[2 * m], x[2 * m + 1]);
+    }
+  } else if constexpr (KIND == FR_DCT4 || KIND == FR_DST4) {
+    const float* xin = static_cast<const float*>(L.in) + (live ? b * L.idist : 0);
+    // x_j of the (DST-IV: reversed) input
+    auto X = [&](int j) { return live ? (KIND == FR_DST4 ? xin[N - 1 - j] : xin[j]) : 0.f; };
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+      const int p = t + T * q;
+      v[q] = cmul(make_float2(X(2 * p), -X(N - 1 - 2 * p)), __ldg(L.post + p));
     }
   } else if constexpr (KIND == FR_DCT3 || KIND == FR_DST3) {
     const float* y = static_cast<const float*>(L.in) + (live ? b * L.idist : 0);
@@ -249,6 +277,8 @@ static cudaError_t run_real_fused_kind(int kind, const RealFusedLaunch& L, cudaS
     case FR_DST2: return run_real_fused<M, E, FR_DST2>(L, st);
     case FR_DCT3: return run_real_fused<M, E, FR_DCT3>(L, st);
     case FR_DST3: return run_real_fused<M, E, FR_DST3>(L, st);
+    case FR_DCT4: return run_real_fused<M, E, FR_DCT4>(L, st);
+    case FR_DST4: return run_real_fused<M, E, FR_DST4>(L, st);
   }
   return cudaErrorInvalidValue;
 }
