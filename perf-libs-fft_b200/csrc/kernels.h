@@ -189,7 +189,8 @@ int group_max_smem_elems();
 
 // Fused single-kernel real transforms for N = 2M, M a power of two
 // (real_fused.cu).  Distances count elements of each buffer's own type.
-enum FusedRealKind { FR_R2C = 0, FR_C2R = 1, FR_DCT2 = 2, FR_DST2 = 3, FR_DCT3 = 4, FR_DST3 = 5, FR_DCT4 = 6, FR_DST4 = 7 };
+enum FusedRealKind { FR_R2C = 0, FR_C2R = 1, FR_DCT2 = 2, FR_DST2 = 3, FR_DCT3 = 4, FR_DST3 = 5, FR_DCT4 = 6, FR_DST4 = 7,
+                     FR_R2HC = 8, FR_HC2R = 9, FR_DHT = 10 };
 struct RealFusedLaunch {
   const void* in;
   void* out;

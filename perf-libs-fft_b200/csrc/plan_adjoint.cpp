@@ -54,7 +54,9 @@ std::unique_ptr<Node> make_adjoint_node(const ConfigData& c, std::string* why) {
         case PLFFT_R2R_DST_4:
           if (auto f = make_real_fused_node(FR_DST4, c.n, lay, scale)) return f;
           return make_realwrap_node(RW_DST4, c.n, lay, scale, why);
-        case PLFFT_R2R_DHT: return make_realwrap_node(RW_DHT, c.n, lay, scale, why);
+        case PLFFT_R2R_DHT:  // self-adjoint
+          if (auto f = make_real_fused_node(FR_DHT, c.n, lay, scale)) return f;
+          return make_realwrap_node(RW_DHT, c.n, lay, scale, why);
         case PLFFT_R2R_R2HC: return make_realwrap_node(RW_HC2R, c.n, lay, scale, why, AW_HC_HALF, AW_NONE);
         case PLFFT_R2R_HC2R: return make_realwrap_node(RW_R2HC, c.n, lay, scale, why, AW_NONE, AW_HC_DOUBLE);
       }

@@ -69,6 +69,9 @@ static std::unique_ptr<Node> make_root(const ConfigData& c, const Layout& lay, b
         if (c.payload == PLFFT_R2R_DST_3) root = make_real_fused_node(FR_DST3, c.n, lay, scale);
         if (c.payload == PLFFT_R2R_DCT_4) root = make_real_fused_node(FR_DCT4, c.n, lay, scale);
         if (c.payload == PLFFT_R2R_DST_4) root = make_real_fused_node(FR_DST4, c.n, lay, scale);
+        if (c.payload == PLFFT_R2R_R2HC) root = make_real_fused_node(FR_R2HC, c.n, lay, scale);
+        if (c.payload == PLFFT_R2R_HC2R) root = make_real_fused_node(FR_HC2R, c.n, lay, scale);
+        if (c.payload == PLFFT_R2R_DHT) root = make_real_fused_node(FR_DHT, c.n, lay, scale);
         if (!root) root = make_realwrap_node(map[c.payload], c.n, lay, scale, why);
         break;
       }

@@ -114,8 +114,8 @@ namespace plfft_b200 {
 
 namespace {
 
-// One-kernel R2C / C2R / DCT-II / DST-II for N = 2M, M a power of two
-// (real_fused.cu); unit element stride.
+// One-kernel R2C / C2R / DCT-II..IV / DST-II..IV / R2HC / HC2R / DHT for
+// N = 2M, M a power of two (real_fused.cu); unit element stride.
 struct RealFusedNode : Node {
   int kind = 0, m = 0;
   RealFusedLaunch base{};
@@ -130,7 +130,8 @@ struct RealFusedNode : Node {
     return launch_real_fused(kind, m, L, st);
   }
   std::string describe() const override {
-    static const char* names[] = {"r2c", "c2r", "dct2", "dst2", "dct3", "dst3", "dct4", "dst4"};
+    static const char* names[] = {"r2c", "c2r",  "dct2", "dst2", "dct3", "dst3",
+                                  "dct4", "dst4", "r2hc", "hc2r", "dht"};
     std::ostringstream o;
     o << "(" << names[kind] << "-fused n=" << 2 * m << " m=" << m << " e=" << base.e << " g=" << base.g
       << ")";

@@ -20,6 +20,9 @@
 // DCT-IV: c_p = (x_{2p} - i x_{N-1-2p}) e^{i pi p/N}, C = backward DFT_M(c),
 //        S_q = e^{i pi (q + 1/4)/N} C_q: y_{2q} = 2 Re S_q, y_{N-1-2q} =
 //        2 Im S_q.  DST-IV(x)_k = (-1)^k DCT-IV(x_{N-1-n})_k.
+// R2HC / HC2R: the R2C / C2R routes with FFTW's half-complex order
+//        (r_0 .. r_M, i_{M-1} .. i_1); DHT: H_k = Re X_k - Im X_k,
+//        H_{N-k} = Re X_k + Im X_k from the R2C route.
 // These are the reference's R2C / C2R twiddle levels
 // (src/level_ab_t_r2c.cpp:17-120, src/level_ab_t_c2r.cpp:17-99) and its
 // DCT-II / DST-II pre/post passes (src/r2r_buffer_helper.hpp:316-335,
@@ -79,7 +82,7 @@ __device__ __forceinline__ void finish_real(float2 (&v)[E], const RealFusedLaunc
       const float u = (f & 1) ? us[N - 1 - (f >> 1)] : us[f >> 1];
       x[f] = (KIND == FR_DST3 && (f & 1)) ? -u * s : u * s;
     }
-  } else if constexpr (KIND == FR_C2R) {
+  } else if constexpr (KIND == FR_C2R || KIND == FR_HC2R) {
     if (!live) return;
     float* x = static_cast<float*>(L.out) + b * L.odist;
 #pragma unroll
@@ -106,6 +109,12 @@ __device__ __forceinline__ void finish_real(float2 (&v)[E], const RealFusedLaunc
       if constexpr (KIND == FR_R2C) {
         const float sk = (L.wmode == 2 && k > 0 && k < M) ? 2.f * s : s;
         static_cast<float2*>(L.out)[b * L.odist + k] = cscale(V, sk);
+      } else if constexpr (KIND == FR_R2HC || KIND == FR_DHT) {
+        float* y = static_cast<float*>(L.out) + b * L.odist;
+        const float re = KIND == FR_R2HC ? V.x : V.x - V.y;
+        const float im = KIND == FR_R2HC ? V.y : V.x + V.y;
+        y[k] = re * s;
+        if (k > 0 && k < M) y[N - k] = im * s;
       } else {
         const float2 c = cmul(__ldg(L.rot + k), V);
         float* y = static_cast<float*>(L.out) + b * L.odist;
@@ -131,7 +140,10 @@ __global__ void __launch_bounds__(pow2_max_threads<E>()) real_fused_kernel(const
   constexpr int T = P::T;
   constexpr int N = 2 * M;
   constexpr int PITCH = (spad_len_c(M) + 1) & ~1;
-  constexpr int DIR = (KIND == FR_C2R || KIND == FR_DCT3 || KIND == FR_DST3 || KIND == FR_DCT4 || KIND == FR_DST4) ? 1 : -1;
+  constexpr int DIR = (KIND == FR_C2R || KIND == FR_HC2R || KIND == FR_DCT3 || KIND == FR_DST3 ||
+                       KIND == FR_DCT4 || KIND == FR_DST4)
+                          ? 1
+                          : -1;
   extern __shared__ __align__(128) unsigned char smraw[];
   const int G = L.g;
   const int grp = threadIdx.x / T;
@@ -147,7 +159,7 @@ __global__ void __launch_bounds__(pow2_max_threads<E>()) real_fused_kernel(const
   };
 
   float2 v[E];
-  if constexpr (KIND == FR_R2C) {
+  if constexpr (KIND == FR_R2C || KIND == FR_R2HC || KIND == FR_DHT) {
     const float* x = static_cast<const float*>(L.in) + (live ? b * L.idist : 0);
 #pragma unroll
     for (int q = 0; q < E; ++q) {
@@ -186,6 +198,23 @@ __global__ void __launch_bounds__(pow2_max_threads<E>()) real_fused_kernel(const
       const bool k0 = k == 0;  // imaginary parts of W_0 and W_M ignored
       xk.y = k0 ? 0.f : xk.y;
       xm.y = k0 ? 0.f : xm.y;
+      const float2 cm = make_float2(xm.x, -xm.y);
+      const float2 a = cadd(xk, cm);
+      const float2 d = csub(xk, cm);
+      const float2 wd = cmulc(d, __ldg(L.post + k));  // conj(W_N^k) * d
+      v[q] = cadd(a, make_float2(-wd.y, wd.x));       // a + i * wd
+    }
+  } else if constexpr (KIND == FR_HC2R) {
+    const float* h = static_cast<const float*>(L.in) + (live ? b * L.idist : 0);
+    // X_j = (r_j, i_j) read from the half-complex order, i_0 = i_M = 0
+    auto Xj = [&](int j) {
+      const bool inner = j > 0 && j < M;
+      return live ? make_float2(h[j], inner ? h[inner ? N - j : 0] : 0.f) : make_float2(0.f, 0.f);
+    };
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+      const int k = t + T * q;
+      const float2 xk = Xj(k), xm = Xj(M - k);
       const float2 cm = make_float2(xm.x, -xm.y);
       const float2 a = cadd(xk, cm);
       const float2 d = csub(xk, cm);
@@ -279,6 +308,9 @@ static cudaError_t run_real_fused_kind(int kind, const RealFusedLaunch& L, cudaS
     case FR_DST3: return run_real_fused<M, E, FR_DST3>(L, st);
     case FR_DCT4: return run_real_fused<M, E, FR_DCT4>(L, st);
     case FR_DST4: return run_real_fused<M, E, FR_DST4>(L, st);
+    case FR_R2HC: return run_real_fused<M, E, FR_R2HC>(L, st);
+    case FR_HC2R: return run_real_fused<M, E, FR_HC2R>(L, st);
+    case FR_DHT: return run_real_fused<M, E, FR_DHT>(L, st);
   }
   return cudaErrorInvalidValue;
 }

@@ -169,9 +169,13 @@ def test_fused_r2c_c2r(n, pad):
     assert oracle.rel_l2(gather(z, hm, rid, n, 1), refz) <= oracle.fp32_tol(n)
 
 
-@pytest.mark.parametrize("kind", ["DCT_2", "DST_2"])
+FUSED_R2R = ["DCT_2", "DST_2", "DCT_3", "DST_3", "DCT_4", "DST_4", "DHT", "R2HC", "HC2R"]
+
+
+@pytest.mark.parametrize("kind", FUSED_R2R)
 @pytest.mark.parametrize("n", [128, 1024, 2048, 4096, 16384])
-def test_fused_dct2_dst2(kind, n):
+def test_fused_r2r(kind, n):
+    """One-kernel R2R kinds for N = 2M, M a power of two (real_fused.cu)."""
     import torch
 
     hm = 3
