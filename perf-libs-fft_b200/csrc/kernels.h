@@ -110,11 +110,12 @@ enum AdjointWeight {
 struct RealWrapLaunch {
   const void* in;
   void* out;
-  float2* work;  // [chunk][len] complex
+  void* work;  // [chunk][len] complex (float2, or double2 when fp64)
   int64_t n, len, nout;
   int64_t istride, idist, ostride, odist;
-  float scale;
+  double scale;
   int wmode_in, wmode_out;
+  int fp64;  // 0: FP32 data, 1: FP64 data
 };
 cudaError_t launch_realwrap(bool pre, int kind, const RealWrapLaunch& L, int64_t m0, int64_t cnt,
                             cudaStream_t st);

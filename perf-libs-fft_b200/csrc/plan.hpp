@@ -148,9 +148,13 @@ std::unique_ptr<Node> make_conv_node(int64_t n, const Layout& lay, int dir, floa
 int64_t next_smooth(int64_t n);
 
 // R2C / C2R / R2R through a C2C plan of a related length (realwrap.cu);
-// kind is a RealWrapKind.
-std::unique_ptr<Node> make_realwrap_node(int kind, int64_t n, const Layout& lay, float scale, std::string* why,
-                                         int wmode_in = 0, int wmode_out = 0);
+// kind is a RealWrapKind.  fp64: double data around an FP64 C2C plan.
+std::unique_ptr<Node> make_realwrap_node(int kind, int64_t n, const Layout& lay, double scale, std::string* why,
+                                         int wmode_in = 0, int wmode_out = 0, bool fp64 = false);
+
+// FP64 C2C node (plan_fp64.cpp); nullptr (with why) for lengths without a
+// schedule.
+std::unique_ptr<Node> make_fp64_c2c(int64_t n, const Layout& lay, int dir, double scale, std::string* why);
 
 // One-kernel R2C / C2R / DCT-II / DST-II (FusedRealKind) for N = 2M, M a
 // power of two in [64, 8192], unit strides; nullptr when not applicable.

@@ -37,6 +37,13 @@ static int64_t span(int64_t howmany, int64_t dist, int64_t n, int64_t stride) {
 
 static std::unique_ptr<Node> make_half_node(const ConfigData& c, const Layout& lay, std::string* why);
 
+// plfft_r2r_kind_t -> RealWrapKind
+static int r2r_wrap_kind(int payload) {
+  static const int map[] = {RW_DCT1, RW_DCT2, RW_DCT3, RW_DCT4, RW_DST1, RW_DST2,
+                            RW_DST3, RW_DST4, RW_DHT,  RW_R2HC, RW_HC2R};
+  return map[payload];
+}
+
 // device schedule for configuration c over the batch layout lay; tune:
 // allow plan-time autotuning (rigor above ESTIMATE)
 static std::unique_ptr<Node> make_root(const ConfigData& c, const Layout& lay, bool tune, std::string* why,
@@ -60,9 +67,6 @@ static std::unique_ptr<Node> make_root(const ConfigData& c, const Layout& lay, b
         if (!root) root = make_realwrap_node(RW_C2R, c.n, lay, scale, why);
         break;
       case TKind::R2R: {
-        // plfft_r2r_kind_t -> RealWrapKind
-        static const int map[] = {RW_DCT1, RW_DCT2, RW_DCT3, RW_DCT4, RW_DST1, RW_DST2,
-                                  RW_DST3, RW_DST4, RW_DHT,  RW_R2HC, RW_HC2R};
         if (c.payload == PLFFT_R2R_DCT_2) root = make_real_fused_node(FR_DCT2, c.n, lay, scale);
         if (c.payload == PLFFT_R2R_DST_2) root = make_real_fused_node(FR_DST2, c.n, lay, scale);
         if (c.payload == PLFFT_R2R_DCT_3) root = make_real_fused_node(FR_DCT3, c.n, lay, scale);
@@ -72,7 +76,7 @@ static std::unique_ptr<Node> make_root(const ConfigData& c, const Layout& lay, b
         if (c.payload == PLFFT_R2R_R2HC) root = make_real_fused_node(FR_R2HC, c.n, lay, scale);
         if (c.payload == PLFFT_R2R_HC2R) root = make_real_fused_node(FR_HC2R, c.n, lay, scale);
         if (c.payload == PLFFT_R2R_DHT) root = make_real_fused_node(FR_DHT, c.n, lay, scale);
-        if (!root) root = make_realwrap_node(map[c.payload], c.n, lay, scale, why);
+        if (!root) root = make_realwrap_node(r2r_wrap_kind(c.payload), c.n, lay, scale, why);
         break;
       }
     }
@@ -80,8 +84,11 @@ static std::unique_ptr<Node> make_root(const ConfigData& c, const Layout& lay, b
     if (c.precision != 0) {
       if (why) *why = "the split-BF16 precision mode takes FP32 data";
     } else {
-      root = make_fp64_node(int(c.kind), c.n, lay, c.kind == TKind::C2C ? c.payload : (c.kind == TKind::R2C ? -1 : 1),
-                            c.scale, why);
+      if (c.kind == TKind::R2R)
+        root = make_realwrap_node(r2r_wrap_kind(c.payload), c.n, lay, c.scale, why, AW_NONE, AW_NONE, true);
+      else
+        root = make_fp64_node(int(c.kind), c.n, lay,
+                              c.kind == TKind::C2C ? c.payload : (c.kind == TKind::R2C ? -1 : 1), c.scale, why);
     }
   } else if (c.data_type == PLFFT_DATA_TYPE_FP16) {
     if (c.precision != 0) {

@@ -14,13 +14,15 @@ struct RealWrapNode : Node {
   int kind = 0;
   int64_t n = 0, len = 0, nout = 0;
   Layout lay{};
-  float scale = 1.f;
+  double scale = 1.0;
   int wmode_in = AW_NONE, wmode_out = AW_NONE;
+  bool fp64 = false;
   int64_t chunk = 1;
+  size_t cbytes() const { return fp64 ? sizeof(double2) : sizeof(float2); }
   std::unique_ptr<Node> inner;  // C2C of length len over `chunk` contiguous members, in place
   size_t inner_ws() const { return inner->workspace(); }
   size_t workspace() const override {
-    const size_t work = size_t(chunk) * size_t(len) * sizeof(float2);
+    const size_t work = size_t(chunk) * size_t(len) * cbytes();
     return ((work + 255) & ~size_t(255)) + inner_ws();
   }
   int launches() const override {
@@ -28,11 +30,11 @@ struct RealWrapNode : Node {
     return int(chunks * (2 + inner->launches()));
   }
   cudaError_t run(const void* in, void* out, void* ws, cudaStream_t st) const override {
-    float2* work = static_cast<float2*>(ws);
-    const size_t work_bytes = (size_t(chunk) * size_t(len) * sizeof(float2) + 255) & ~size_t(255);
+    void* work = ws;
+    const size_t work_bytes = (size_t(chunk) * size_t(len) * cbytes() + 255) & ~size_t(255);
     void* iws = static_cast<char*>(ws) + work_bytes;
-    RealWrapLaunch L{in, out, work, n, len, nout, lay.istride, lay.idist, lay.ostride, lay.odist, scale,
-                     wmode_in, wmode_out};
+    RealWrapLaunch L{in,        out,       work,     n,          len,        nout, lay.istride, lay.idist, lay.ostride,
+                     lay.odist, scale,     wmode_in, wmode_out, fp64 ? 1 : 0};
     for (int64_t m0 = 0; m0 < lay.howmany; m0 += chunk) {
       const int64_t cnt = std::min(chunk, lay.howmany - m0);
       cudaError_t e = launch_realwrap(true, kind, L, m0, cnt, st);
@@ -46,14 +48,14 @@ struct RealWrapNode : Node {
   }
   // the inner plan was built for `chunk` members; the last chunk may be
   // shorter, which only changes which members hold meaningful data
-  cudaError_t run_inner(int64_t, float2* work, void* iws, cudaStream_t st) const {
+  cudaError_t run_inner(int64_t, void* work, void* iws, cudaStream_t st) const {
     return inner->run(work, work, iws, st);
   }
   std::string describe() const override {
     static const char* names[] = {"r2c", "c2r", "dct1", "dct2", "dct3", "dct4", "dst1",
                                   "dst2", "dst3", "dst4", "dht", "r2hc", "hc2r"};
     std::ostringstream o;
-    o << "(" << names[kind] << "-via-c2c n=" << n << " len=" << len << " chunk=" << chunk << " "
+    o << "(" << names[kind] << (fp64 ? "-fp64" : "") << "-via-c2c n=" << n << " len=" << len << " chunk=" << chunk << " "
       << inner->describe() << ")";
     return o.str();
   }
@@ -85,8 +87,8 @@ int wrap_dir(int kind) {
 
 }  // namespace
 
-std::unique_ptr<Node> make_realwrap_node(int kind, int64_t n, const Layout& lay, float scale, std::string* why,
-                                         int wmode_in, int wmode_out) {
+std::unique_ptr<Node> make_realwrap_node(int kind, int64_t n, const Layout& lay, double scale, std::string* why,
+                                         int wmode_in, int wmode_out, bool fp64) {
   if (kind == RW_DCT1 && n < 2) {
     if (why) *why = "DCT-I needs n > 1";
     return nullptr;
@@ -100,10 +102,12 @@ std::unique_ptr<Node> make_realwrap_node(int kind, int64_t n, const Layout& lay,
   node->scale = scale;
   node->wmode_in = wmode_in;
   node->wmode_out = wmode_out;
+  node->fp64 = fp64;
   const int64_t target = 64ll << 20;  // bytes of complex work per chunk
-  node->chunk = std::max<int64_t>(1, std::min<int64_t>(lay.howmany, target / (node->len * 8)));
+  node->chunk = std::max<int64_t>(1, std::min<int64_t>(lay.howmany, target / (node->len * int64_t(node->cbytes()))));
   Layout inner{node->chunk, 1, node->len, 1, node->len};
-  node->inner = make_c2c_node(node->len, inner, wrap_dir(kind), 1.0f, 0, why);
+  node->inner = fp64 ? make_fp64_c2c(node->len, inner, wrap_dir(kind), 1.0, why)
+                     : make_c2c_node(node->len, inner, wrap_dir(kind), 1.0f, 0, why);
   if (!node->inner) return nullptr;
   return node;
 }

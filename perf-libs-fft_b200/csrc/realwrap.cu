@@ -22,7 +22,8 @@
 //   HC2R     N        F from the half-complex layout          Re F_k        (backward)
 //
 // This generic path serves every length the C2C planner supports (on-chip,
-// four-step, Rader, Bluestein).  The reference builds the same kinds as a
+// four-step, Rader, Bluestein), for FP32 data and, around the FP64 C2C
+// plans, for FP64 data (the R2R kinds in double).  The reference builds the same kinds as a
 // permuted R2C/C2R/C2C plus O(n) pre/post passes (src/r2r_plan.cpp:15-79,
 // src/r2r_buffer_helper.hpp:231-1026); the fused single-kernel paths for the
 // hot kinds live in real_fused.cu.
@@ -33,17 +34,37 @@
 
 namespace plfft_b200 {
 
-// e^{i * sign * pi * num / den}, computed from the table of W_{4N}^m or
-// directly in double for the few entries per element (FP64 is used only for
-// these constants).
-__device__ __forceinline__ float2 expi_pi(int64_t num, int64_t den) {
-  // angle = pi * num / den, reduced modulo 2 pi in integers
+// complex type of a real type, built component-wise so one kernel body
+// serves FP32 (float2) and FP64 (double2) data
+template <class R>
+struct CplxOf;
+template <>
+struct CplxOf<float> {
+  using type = float2;
+};
+template <>
+struct CplxOf<double> {
+  using type = double2;
+};
+
+template <class R>
+__device__ __forceinline__ typename CplxOf<R>::type cx(R re, R im) {
+  typename CplxOf<R>::type z;
+  z.x = re;
+  z.y = im;
+  return z;
+}
+
+// e^{i pi num / den}: the angle reduced modulo 2 pi in integers, evaluated
+// in double (FP32 data rounds the result once)
+template <class R>
+__device__ __forceinline__ typename CplxOf<R>::type expi_pi(int64_t num, int64_t den) {
   const int64_t per = 2 * den;
   int64_t m = num % per;
   if (m < 0) m += per;
   double s, c;
   sincospi(double(m) / double(den), &s, &c);
-  return make_float2(float(c), float(s));
+  return cx<R>(R(c), R(s));
 }
 
 // weight of element j (length n) under an AdjointWeight mode
@@ -63,97 +84,98 @@ __device__ __forceinline__ float adj_weight(int mode, int64_t j, int64_t n) {
   }
 }
 
-template <int KIND>
-__device__ __forceinline__ float load_real(const RealWrapLaunch& L, int64_t b, int64_t j) {
-  const float v = static_cast<const float*>(L.in)[b * L.idist + j * L.istride];
-  return L.wmode_in ? v * adj_weight(L.wmode_in, j, L.n) : v;
+template <class R>
+__device__ __forceinline__ R load_real(const RealWrapLaunch& L, int64_t b, int64_t j) {
+  const R v = static_cast<const R*>(L.in)[b * L.idist + j * L.istride];
+  return L.wmode_in ? v * R(adj_weight(L.wmode_in, j, L.n)) : v;
 }
 
-template <int KIND>
+template <class R, int KIND>
 __global__ void __launch_bounds__(256) realwrap_pre(const RealWrapLaunch L, int64_t m0, int64_t cnt) {
+  using C = typename CplxOf<R>::type;
   const int64_t n = L.n, len = L.len;
   const int64_t total = cnt * len;
+  C* work = static_cast<C*>(L.work);
   for (int64_t f = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; f < total; f += int64_t(gridDim.x) * blockDim.x) {
     const int64_t bl = f / len;
     const int64_t j = f - bl * len;
     const int64_t b = m0 + bl;
-    float2 z = make_float2(0.f, 0.f);
+    C z = cx<R>(0, 0);
     if constexpr (KIND == RW_R2C || KIND == RW_DHT || KIND == RW_R2HC) {
-      z.x = load_real<KIND>(L, b, j);
+      z.x = load_real<R>(L, b, j);
     } else if constexpr (KIND == RW_C2R) {
-      const float2* X = static_cast<const float2*>(L.in) + b * L.idist;
+      const C* X = static_cast<const C*>(L.in) + b * L.idist;
       const int64_t h = n / 2;
-      if (j <= h) {
-        z = X[j * L.istride];
-        if (j == 0 || (2 * j == n)) z.y = 0.f;
-        if (L.wmode_in) z = cscale(z, adj_weight(L.wmode_in, j, n));
-      } else {
-        const float2 c = X[(n - j) * L.istride];
-        z = make_float2(c.x, -c.y);
-        if (L.wmode_in) z = cscale(z, adj_weight(L.wmode_in, n - j, n));
-      }
+      const int64_t src = j <= h ? j : n - j;
+      const C v = X[src * L.istride];
+      const R w = L.wmode_in ? R(adj_weight(L.wmode_in, src, n)) : R(1);
+      if (j <= h)
+        z = cx<R>(v.x * w, (j == 0 || 2 * j == n) ? R(0) : v.y * w);
+      else
+        z = cx<R>(v.x * w, -v.y * w);
     } else if constexpr (KIND == RW_HC2R) {
       const int64_t h = n / 2;
       if (j == 0) {
-        z.x = load_real<KIND>(L, b, 0);
+        z.x = load_real<R>(L, b, 0);
       } else if (2 * j == n) {
-        z.x = load_real<KIND>(L, b, h);
+        z.x = load_real<R>(L, b, h);
       } else if (j <= h) {
-        z = make_float2(load_real<KIND>(L, b, j), load_real<KIND>(L, b, n - j));
+        z = cx<R>(load_real<R>(L, b, j), load_real<R>(L, b, n - j));
       } else {
-        z = make_float2(load_real<KIND>(L, b, n - j), -load_real<KIND>(L, b, j));
+        z = cx<R>(load_real<R>(L, b, n - j), -load_real<R>(L, b, j));
       }
     } else if constexpr (KIND == RW_DCT1) {
       const int64_t src = j < n ? j : len - j;
-      z.x = load_real<KIND>(L, b, src);
+      z.x = load_real<R>(L, b, src);
     } else if constexpr (KIND == RW_DCT2) {
       const int64_t src = j < n ? j : 2 * n - 1 - j;
-      z.x = load_real<KIND>(L, b, src);
+      z.x = load_real<R>(L, b, src);
     } else if constexpr (KIND == RW_DST2) {
-      z.x = j < n ? load_real<KIND>(L, b, j) : -load_real<KIND>(L, b, 2 * n - 1 - j);
+      z.x = j < n ? load_real<R>(L, b, j) : -load_real<R>(L, b, 2 * n - 1 - j);
     } else if constexpr (KIND == RW_DST1) {
-      if (j >= 1 && j <= n) z.x = load_real<KIND>(L, b, j - 1);
-      else if (j >= n + 2) z.x = -load_real<KIND>(L, b, len - j - 1);
+      if (j >= 1 && j <= n) z.x = load_real<R>(L, b, j - 1);
+      else if (j >= n + 2) z.x = -load_real<R>(L, b, len - j - 1);
     } else if constexpr (KIND == RW_DCT3) {
       if (j < n) {
-        const float x = load_real<KIND>(L, b, j) * (j == 0 ? 1.f : 2.f);
-        const float2 w = expi_pi(j, 2 * n);
-        z = make_float2(x * w.x, x * w.y);
+        const R x = load_real<R>(L, b, j) * (j == 0 ? R(1) : R(2));
+        const C w = expi_pi<R>(j, 2 * n);
+        z = cx<R>(x * w.x, x * w.y);
       }
     } else if constexpr (KIND == RW_DST3) {
       if (j >= 1 && j <= n) {
-        const float x = load_real<KIND>(L, b, j - 1) * (j == n ? 1.f : 2.f);
-        const float2 w = expi_pi(j, 2 * n);
-        z = make_float2(x * w.x, x * w.y);
+        const R x = load_real<R>(L, b, j - 1) * (j == n ? R(1) : R(2));
+        const C w = expi_pi<R>(j, 2 * n);
+        z = cx<R>(x * w.x, x * w.y);
       }
     } else if constexpr (KIND == RW_DCT4 || KIND == RW_DST4) {
       if (j < n) {
-        const float x = load_real<KIND>(L, b, j);
-        const float2 w = expi_pi(-j, 2 * n);
-        z = make_float2(x * w.x, x * w.y);
+        const R x = load_real<R>(L, b, j);
+        const C w = expi_pi<R>(-j, 2 * n);
+        z = cx<R>(x * w.x, x * w.y);
       }
     }
-    L.work[bl * len + j] = z;
+    work[bl * len + j] = z;
   }
 }
 
-template <int KIND>
+template <class R, int KIND>
 __global__ void __launch_bounds__(256) realwrap_post(const RealWrapLaunch L, int64_t m0, int64_t cnt) {
+  using C = typename CplxOf<R>::type;
   const int64_t n = L.n, len = L.len, nout = L.nout;
   const int64_t total = cnt * nout;
-  const float s = L.scale;
+  const R s = R(L.scale);
   for (int64_t f = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; f < total; f += int64_t(gridDim.x) * blockDim.x) {
     const int64_t bl = f / nout;
     const int64_t k = f - bl * nout;
     const int64_t b = m0 + bl;
-    const float2* F = L.work + bl * len;
+    const C* F = static_cast<const C*>(L.work) + bl * len;
     if constexpr (KIND == RW_R2C) {
-      float2* Y = static_cast<float2*>(L.out) + b * L.odist;
-      const float2 v = F[k];
-      const float sw = L.wmode_out ? s * adj_weight(L.wmode_out, k, n) : s;
-      Y[k * L.ostride] = make_float2(v.x * sw, v.y * sw);
+      C* Y = static_cast<C*>(L.out) + b * L.odist;
+      const C v = F[k];
+      const R sw = L.wmode_out ? s * R(adj_weight(L.wmode_out, k, n)) : s;
+      Y[k * L.ostride] = cx<R>(v.x * sw, v.y * sw);
     } else {
-      float y = 0.f;
+      R y = 0;
       if constexpr (KIND == RW_C2R || KIND == RW_HC2R || KIND == RW_DCT1 || KIND == RW_DCT3) {
         y = F[k].x;
       } else if constexpr (KIND == RW_DST3) {
@@ -163,44 +185,46 @@ __global__ void __launch_bounds__(256) realwrap_post(const RealWrapLaunch L, int
       } else if constexpr (KIND == RW_R2HC) {
         y = (k <= n / 2) ? F[k].x : F[n - k].y;
       } else if constexpr (KIND == RW_DCT2) {
-        const float2 w = expi_pi(-k, 2 * n);
+        const C w = expi_pi<R>(-k, 2 * n);
         y = F[k].x * w.x - F[k].y * w.y;
       } else if constexpr (KIND == RW_DST2) {
-        const float2 w = expi_pi(-(k + 1), 2 * n);
-        const float2 v = F[k + 1];
+        const C w = expi_pi<R>(-(k + 1), 2 * n);
+        const C v = F[k + 1];
         y = -(v.x * w.y + v.y * w.x);
       } else if constexpr (KIND == RW_DST1) {
         y = -F[k + 1].y;
       } else if constexpr (KIND == RW_DCT4 || KIND == RW_DST4) {
-        const float2 w = expi_pi(-(2 * k + 1), 4 * n);
-        const float2 v = F[k];
+        const C w = expi_pi<R>(-(2 * k + 1), 4 * n);
+        const C v = F[k];
         if constexpr (KIND == RW_DCT4)
-          y = 2.f * (v.x * w.x - v.y * w.y);
+          y = R(2) * (v.x * w.x - v.y * w.y);
         else
-          y = -2.f * (v.x * w.y + v.y * w.x);
+          y = R(-2) * (v.x * w.y + v.y * w.x);
       }
-      const float sw = L.wmode_out ? s * adj_weight(L.wmode_out, k, n) : s;
-      static_cast<float*>(L.out)[b * L.odist + k * L.ostride] = y * sw;
+      const R sw = L.wmode_out ? s * R(adj_weight(L.wmode_out, k, n)) : s;
+      static_cast<R*>(L.out)[b * L.odist + k * L.ostride] = y * sw;
     }
   }
 }
 
-template <int KIND>
+template <class R, int KIND>
 static cudaError_t run_pre_post(bool pre, const RealWrapLaunch& L, int64_t m0, int64_t cnt, cudaStream_t st) {
   const int64_t total = cnt * (pre ? L.len : L.nout);
-  const int64_t blocks = std::min<int64_t>((total + 255) / 256, 148 * 16);
+  const unsigned blocks = unsigned(std::max<int64_t>(std::min<int64_t>((total + 255) / 256, 148 * 16), 1));
   if (pre)
-    realwrap_pre<KIND><<<unsigned(std::max<int64_t>(blocks, 1)), 256, 0, st>>>(L, m0, cnt);
+    realwrap_pre<R, KIND><<<blocks, 256, 0, st>>>(L, m0, cnt);
   else
-    realwrap_post<KIND><<<unsigned(std::max<int64_t>(blocks, 1)), 256, 0, st>>>(L, m0, cnt);
+    realwrap_post<R, KIND><<<blocks, 256, 0, st>>>(L, m0, cnt);
   return cudaGetLastError();
 }
 
-cudaError_t launch_realwrap(bool pre, int kind, const RealWrapLaunch& L, int64_t m0, int64_t cnt, cudaStream_t st) {
+template <class R>
+static cudaError_t launch_realwrap_t(bool pre, int kind, const RealWrapLaunch& L, int64_t m0, int64_t cnt,
+                                     cudaStream_t st) {
   switch (kind) {
 #define PLFFT_B200_RW(K) \
   case K:                \
-    return run_pre_post<K>(pre, L, m0, cnt, st);
+    return run_pre_post<R, K>(pre, L, m0, cnt, st);
     PLFFT_B200_RW(RW_R2C)
     PLFFT_B200_RW(RW_C2R)
     PLFFT_B200_RW(RW_DCT1)
@@ -217,6 +241,11 @@ cudaError_t launch_realwrap(bool pre, int kind, const RealWrapLaunch& L, int64_t
 #undef PLFFT_B200_RW
   }
   return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_realwrap(bool pre, int kind, const RealWrapLaunch& L, int64_t m0, int64_t cnt, cudaStream_t st) {
+  return L.fp64 ? launch_realwrap_t<double>(pre, kind, L, m0, cnt, st)
+                : launch_realwrap_t<float>(pre, kind, L, m0, cnt, st);
 }
 
 }  // namespace plfft_b200

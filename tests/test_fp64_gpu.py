@@ -65,12 +65,44 @@ def test_fp64_r2c_c2r(n):
     assert oracle.rel_l2(back.reshape(hm, n), n * x) <= 1e-11, plan2.describe()
 
 
-def test_fp64_r2r_fails_plan_creation():
-    import plfft
+R2R = ["DCT_1", "DCT_2", "DCT_3", "DCT_4", "DST_1", "DST_2", "DST_3", "DST_4", "DHT", "R2HC", "HC2R"]
 
-    with pytest.raises(plfft.PlfftError) as e:
-        plfft.make_plan("r2r", 64, 1, r2r_kind=plfft.R2RKind.DCT_2, data_type=plfft.DataType.FP64)
-    assert e.value.status == plfft.Status.PLAN_CREATION_FAILED
+
+@pytest.mark.parametrize("kind", R2R)
+@pytest.mark.parametrize("n", [2, 17, 64, 1000])
+def test_fp64_r2r(kind, n):
+    """Every R2R kind in FP64: double pre/post passes around the FP64 C2C."""
+    import plfft
+    import torch
+
+    rng = np.random.default_rng(hash((kind, n)) % 2**32)
+    hm = 3
+    x = rng.uniform(-1, 1, (hm, n))
+    plan = plfft.make_plan("r2r", n, hm, r2r_kind=plfft.R2RKind[kind], data_type=plfft.DataType.FP64)
+    assert "fp64" in plan.describe(), plan.describe()
+    d_in = torch.from_numpy(x.ravel().copy()).cuda()
+    d_out = torch.zeros(hm * n, dtype=torch.float64, device="cuda")
+    plan.execute(d_in.data_ptr(), d_out.data_ptr())
+    ref = oracle.r2r(x, kind)
+    assert oracle.rel_l2(d_out.cpu().numpy().reshape(hm, n), ref) <= tol64(2 * n), plan.describe()
+
+
+def test_fp64_r2r_strided_scaled():
+    import plfft
+    import torch
+
+    n, hm, is_, os_ = 64, 2, 2, 3
+    rng = np.random.default_rng(11)
+    x = rng.uniform(-1, 1, (hm, n))
+    buf = np.zeros(hm * n * is_)
+    buf[np.arange(hm)[:, None] * n * is_ + np.arange(n)[None, :] * is_] = x
+    plan = plfft.make_plan("r2r", n, hm, is_, n * is_, os_, n * os_, r2r_kind=plfft.R2RKind.DST_2,
+                           data_type=plfft.DataType.FP64, scale=0.25)
+    d_in = torch.from_numpy(buf).cuda()
+    d_out = torch.zeros(hm * n * os_, dtype=torch.float64, device="cuda")
+    plan.execute(d_in.data_ptr(), d_out.data_ptr())
+    got = d_out.cpu().numpy()[np.arange(hm)[:, None] * n * os_ + np.arange(n)[None, :] * os_]
+    assert oracle.rel_l2(got, 0.25 * oracle.r2r(x, "DST_2")) <= tol64(2 * n)
 
 
 @pytest.mark.parametrize("n", [1024, 3 * 4096, 97])
