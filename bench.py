@@ -424,7 +424,7 @@ def make_workload(name):
                                                 "c2c", 1024, 4096, profile="c2c_pow2_n1024_b4096"),
         "r2c_c2r_n4096_b8192": lambda: RoundTripWorkload("r2c_c2r_n4096_b8192",
                                                          "R2C + C2R(1/N) FP32 round trip N=4096 batch=8192",
-                                                         4096, 8192),
+                                                         4096, 8192, profile="real_fused_n4096_b8192"),
         "dct2_n1024_b4096": lambda: PlanWorkload("dct2_n1024_b4096", "R2R DCT-II FP32 N=1024 batch=4096", "r2r",
                                                  1024, 4096, r2r="DCT_2"),
         "dst2_n1024_b4096": lambda: PlanWorkload("dst2_n1024_b4096", "R2R DST-II FP32 N=1024 batch=4096", "r2r",
