@@ -202,6 +202,7 @@ struct RealFusedLaunch {
   const float2* post;  // W_N^k, k = 0..M (DCT-IV / DST-IV: exp(i pi p / N), p < M)
   const float2* rot;   // exp(-i pi k / 2N), k = 0..M (DCT-IV / DST-IV: exp(i pi (4q+1) / 4N), q < M)
   int pairs_in, pairs_out;  // real data may be moved as aligned float pairs
+  int quads_in;             // real input may be read as aligned float4
   int e;                    // elements per thread of the length-M FFT
   int wmode;                // adjoint weights: 1 C2R input bins 0<k<M times 1/2,
                             // 2 R2C output bins 0<k<M times 2, 3 DCT-III input

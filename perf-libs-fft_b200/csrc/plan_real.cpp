@@ -131,6 +131,7 @@ struct RealFusedNode : Node {
     const bool in_real = kind != FR_C2R, out_real = kind != FR_R2C;
     L.pairs_in = in_real && (reinterpret_cast<uintptr_t>(in) % 8 == 0) && (L.howmany == 1 || L.idist % 2 == 0);
     L.pairs_out = out_real && (reinterpret_cast<uintptr_t>(out) % 8 == 0) && (L.howmany == 1 || L.odist % 2 == 0);
+    L.quads_in = in_real && (reinterpret_cast<uintptr_t>(in) % 16 == 0) && (L.howmany == 1 || L.idist % 4 == 0);
     return launch_real_fused(kind, m, L, st);
   }
   std::string describe() const override {
@@ -185,6 +186,7 @@ std::unique_ptr<Node> make_real_fused_node(int kind, int64_t n, const Layout& la
   node->base.odist = lay.odist;
   node->base.g = std::max(1, 128 / t);
   if (const char* v = std::getenv("PLFFT_B200_RF_G")) node->base.g = std::max(1, std::atoi(v));
+  node->base.g = std::max(node->base.g, std::max(1, 32 / t));  // whole warps (the kernel shuffles)
   node->base.e = e;
   node->base.wmode = wmode;
   node->base.scale = scale;

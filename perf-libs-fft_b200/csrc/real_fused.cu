@@ -32,16 +32,19 @@
 
 namespace plfft_b200 {
 
-// V_k (k = 0..M) of the real length-2M input from Z = DFT_M(z) held in
-// natural order in shared memory
-__device__ __forceinline__ float2 real_split(const float2* Z, int k, int m, const float2* post) {
-  const float2 zk = Z[k == m ? 0 : k];
-  const float2 zm = Z[k == 0 ? 0 : m - k];
+// V_k of the real length-2M input from zk = Z_k and zm = Z_{M-k}
+// (Z = DFT_M(z), indices mod M) and w = W_N^k
+__device__ __forceinline__ float2 split_pair(float2 zk, float2 zm, float2 w) {
   const float2 cm = make_float2(zm.x, -zm.y);
   const float2 e = cscale(cadd(zk, cm), 0.5f);
   const float2 o = cscale(csub(zk, cm), 0.5f);
-  const float2 wo = cmul(__ldg(post + k), o);
+  const float2 wo = cmul(w, o);
   return make_float2(e.x + wo.y, e.y - wo.x);  // e - i * wo
+}
+
+// V_k (k = 0..M) from Z held in natural order in shared memory
+__device__ __forceinline__ float2 real_split(const float2* Z, int k, int m, const float2* post) {
+  return split_pair(Z[k == m ? 0 : k], Z[k == 0 ? 0 : m - k], __ldg(post + k));
 }
 
 template <int M, int E, int KIND, class Sync>
@@ -97,15 +100,8 @@ __device__ __forceinline__ void finish_real(float2 (&v)[E], const RealFusedLaunc
       }
     }
   } else {
-    sync();  // last exchange fully read
-#pragma unroll
-    for (int q = 0; q < E; ++q) mine[t + T * q] = v[q];
-    sync();
-    if (!live) return;
-    // k = t + T*j for j < E covers 0..M-1 (unrolled, so the table loads
-    // of all j are in flight together); thread 0 also takes k = M
-    auto out_k = [&](int k) {
-      const float2 V = real_split(mine, k, M, L.post);
+    // outputs of bin k from V_k (k = 0..M)
+    auto emit = [&](int k, float2 V) {
       if constexpr (KIND == FR_R2C) {
         const float sk = (L.wmode == 2 && k > 0 && k < M) ? 2.f * s : s;
         static_cast<float2*>(L.out)[b * L.odist + k] = cscale(V, sk);
@@ -128,9 +124,16 @@ __device__ __forceinline__ void finish_real(float2 (&v)[E], const RealFusedLaunc
         }
       }
     };
+    sync();  // last exchange fully read
 #pragma unroll
-    for (int j = 0; j < E; ++j) out_k(t + T * j);
-    if (t == 0) out_k(M);
+    for (int q = 0; q < E; ++q) mine[t + T * q] = v[q];
+    sync();
+    if (!live) return;
+    // k = t + T*j for j < E covers 0..M-1 (unrolled, so the table loads
+    // of all j are in flight together); thread 0 also takes k = M
+#pragma unroll
+    for (int j = 0; j < E; ++j) emit(t + T * j, real_split(mine, t + T * j, M, L.post));
+    if (t == 0) emit(M, real_split(mine, M, M, L.post));
   }
 }
 
@@ -244,6 +247,23 @@ __global__ void __launch_bounds__(pow2_max_threads<E>()) real_fused_kernel(const
       const float2 d = csub(xk, cm);
       const float2 wd = cmulc(d, __ldg(L.post + k));  // conj(W_N^k) * d
       v[q] = cadd(a, make_float2(-wd.y, wd.x));       // a + i * wd
+    }
+  } else if (T <= 32 && L.quads_in) {  // T is a compile-time constant
+    // DCT-II / DST-II from aligned float4 loads, no staging: x_{4m..4m+3}
+    // (m < M/2) holds z_m = (x_{4m}, x_{4m+2}) and z_{M-1-m} = (x_{4m+3},
+    // x_{4m+1}) of the Makhoul-permuted pairs.  For m = t + T q, z_{M-1-m}
+    // is element E-1-q of lane T-1-t (t XOR (T-1), same warp as T <= 32),
+    // so the two lanes swap those halves with one shuffle per component.
+    const float4* x4 = reinterpret_cast<const float4*>(static_cast<const float*>(L.in) + (live ? b * L.idist : 0));
+#pragma unroll
+    for (int q = 0; q < E / 2; ++q) {
+      float4 a = live ? x4[t + T * q] : make_float4(0.f, 0.f, 0.f, 0.f);
+      if constexpr (KIND == FR_DST2) {
+        a.y = -a.y;
+        a.w = -a.w;
+      }
+      v[q] = make_float2(a.x, a.z);
+      v[E - 1 - q] = make_float2(__shfl_xor_sync(0xffffffffu, a.w, T - 1), __shfl_xor_sync(0xffffffffu, a.y, T - 1));
     }
   } else {
     // DCT-II / DST-II: stage the N reals in the slot, then gather the
