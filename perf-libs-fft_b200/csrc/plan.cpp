@@ -822,6 +822,9 @@ PlanData::~PlanData() {
   if (stream) cudaStreamDestroy(stream);
   for (auto& st : pipe_st)
     if (st) cudaStreamDestroy(st);
+  for (auto& row : pipe_ev)
+    for (auto& ev : row)
+      if (ev) cudaEventDestroy(ev);
 }
 
 }  // namespace plfft_b200

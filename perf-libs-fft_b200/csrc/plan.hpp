@@ -186,13 +186,17 @@ struct PlanData {
   std::string tune_note;                // how the schedule was chosen (rigor > ESTIMATE)
   int64_t nin = 0, nout = 0;            // logical elements per member
   // host-buffer pipeline (plfft_plan_execute on host pointers): the batch in
-  // chunks whose copies and kernels overlap across streams; built on first use
+  // chunks that flow through three streams (host-to-device copies, kernels,
+  // device-to-host copies) ordered by one event pair per chunk, so each copy
+  // direction streams back to back; built on first use
   static constexpr int kPipeStreams = 3;
+  static constexpr int kPipeMaxChunks = 64;
   mutable bool pipe_built = false;
   mutable int64_t pipe_per = 0;  // members per chunk, 0 = no pipeline
   mutable std::unique_ptr<Node> pipe_node, pipe_tail;
   mutable cudaStream_t pipe_st[kPipeStreams] = {};
-  mutable DevBuf pipe_ws[kPipeStreams];
+  mutable cudaEvent_t pipe_ev[2][kPipeMaxChunks] = {};
+  mutable DevBuf pipe_ws;
   ~PlanData();
 };
 

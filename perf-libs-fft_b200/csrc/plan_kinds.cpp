@@ -223,6 +223,10 @@ static cudaError_t ensure(DevBuf& b, size_t bytes) {
 
 // Chunked schedules for host-buffer execution, built once (plan mutex held).
 // Chunks need members whose spans do not interleave and a dense output.
+// (measured on a 64 MiB C2C: chunks of 1 / 2 / 4 / 8 / 16 MiB of traffic
+// gave 49 / 53 / 62 / 72 / 73 GB/s end to end)
+constexpr int64_t kPipeChunkMb = 16;
+
 static void build_pipe(const PlanData& p) {
   p.pipe_built = true;
   const ConfigData& c = p.cfg;
@@ -230,14 +234,12 @@ static void build_pipe(const PlanData& p) {
   if (c.howmany < 4 || !p.out_dense || c.istride < 1 || c.ostride < 1) return;
   if (c.idist < (p.nin - 1) * c.istride + 1 || c.odist < (p.nout - 1) * c.ostride + 1) return;
   if (ib + ob < (int64_t(16) << 20)) return;  // too small to gain from overlap
-  // chunks of about 16 MiB of traffic on three streams: the host-to-device
-  // copy of one chunk, the kernels of another and the device-to-host copy
-  // of a third overlap (measured for 64 MiB: 2 / 4 / 8 / 16 / 32 MiB chunks
-  // gave 56 / 61 / 67 / 72 / 67 GB/s end to end; concurrent pinned copies
-  // alone reach 95 GB/s)
-  int64_t chunk_mb = 16;
+  // chunks of about 16 MiB of traffic: the host-to-device copy of chunk i+1,
+  // the kernels of chunk i and the device-to-host copy of chunk i-1 overlap
+  // (concurrent pinned copies in both directions reach about 95 GB/s)
+  int64_t chunk_mb = kPipeChunkMb;
   if (const char* v = std::getenv("PLFFT_B200_PIPE_MB")) chunk_mb = std::max(1, std::atoi(v));
-  const int64_t k = std::min<int64_t>(64, std::max<int64_t>(2, (ib + ob) / (chunk_mb << 20)));
+  const int64_t k = std::min<int64_t>(PlanData::kPipeMaxChunks, std::max<int64_t>(2, (ib + ob) / (chunk_mb << 20)));
   const int64_t per = (c.howmany + k - 1) / k;
   const int64_t tail = c.howmany - (c.howmany - 1) / per * per;
   std::string why, note;
@@ -246,13 +248,22 @@ static void build_pipe(const PlanData& p) {
   if (!p.pipe_node || (tail != per && !p.pipe_tail)) return;
   size_t ws = p.pipe_node->workspace();
   if (p.pipe_tail) ws = std::max(ws, p.pipe_tail->workspace());
-  for (int i = 0; i < PlanData::kPipeStreams; ++i) {
-    if (cudaStreamCreateWithFlags(&p.pipe_st[i], cudaStreamNonBlocking) != cudaSuccess ||
-        p.pipe_ws[i].alloc(ws) != cudaSuccess) {
+  if (p.pipe_ws.alloc(ws) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  for (auto& st : p.pipe_st)
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
       cudaGetLastError();
       return;
     }
-  }
+  const int64_t chunks = (c.howmany + per - 1) / per;
+  for (auto& row : p.pipe_ev)
+    for (int64_t i = 0; i < chunks; ++i)
+      if (cudaEventCreateWithFlags(&row[i], cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+      }
   p.pipe_per = per;
 }
 
@@ -262,18 +273,22 @@ static cudaError_t execute_pipelined(const PlanData& p, const void* in, void* ou
   auto* hout = static_cast<unsigned char*>(out);
   auto* din = static_cast<unsigned char*>(p.stage_in.p);
   auto* dout = static_cast<unsigned char*>(p.stage_out.p);
+  cudaStream_t s_in = p.pipe_st[0], s_k = p.pipe_st[1], s_out = p.pipe_st[2];
   cudaError_t e = cudaSuccess;
   int i = 0;
   for (int64_t m0 = 0; m0 < c.howmany && e == cudaSuccess; m0 += p.pipe_per, ++i) {
     const int64_t cnt = std::min(p.pipe_per, c.howmany - m0);
     const Node& node = cnt == p.pipe_per ? *p.pipe_node : *p.pipe_tail;
-    cudaStream_t st = p.pipe_st[i % PlanData::kPipeStreams];
     const size_t ioff = size_t(m0 * c.idist) * p.in_bytes, ooff = size_t(m0 * c.odist) * p.out_bytes;
     const size_t ilen = size_t(span(cnt, c.idist, p.nin, c.istride)) * p.in_bytes;
     const size_t olen = size_t(span(cnt, c.odist, p.nout, c.ostride)) * p.out_bytes;
-    e = cudaMemcpyAsync(din + ioff, hin + ioff, ilen, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = node.run(din + ioff, dout + ooff, p.pipe_ws[i % PlanData::kPipeStreams].p, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(hout + ooff, dout + ooff, olen, cudaMemcpyDeviceToHost, st);
+    e = cudaMemcpyAsync(din + ioff, hin + ioff, ilen, cudaMemcpyHostToDevice, s_in);
+    if (e == cudaSuccess) e = cudaEventRecord(p.pipe_ev[0][i], s_in);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s_k, p.pipe_ev[0][i], 0);
+    if (e == cudaSuccess) e = node.run(din + ioff, dout + ooff, p.pipe_ws.p, s_k);
+    if (e == cudaSuccess) e = cudaEventRecord(p.pipe_ev[1][i], s_k);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s_out, p.pipe_ev[1][i], 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hout + ooff, dout + ooff, olen, cudaMemcpyDeviceToHost, s_out);
   }
   for (auto st : p.pipe_st) {
     const cudaError_t s = cudaStreamSynchronize(st);
