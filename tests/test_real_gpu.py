@@ -188,22 +188,24 @@ def test_fused_r2r(kind, n):
     assert oracle.rel_l2(y, ref) <= oracle.fp32_tol(2 * n)
 
 
-@pytest.mark.parametrize("kind", ["DCT_2", "DST_2"])
+@pytest.mark.parametrize("kind", ["DCT_2", "DST_2", "DCT_3", "DST_3"])
 @pytest.mark.parametrize("n", [128, 1024, 2048])
 @pytest.mark.parametrize("pad", [0, 1, 2, 4])
-def test_fused_dct2_member_alignment(kind, n, pad):
-    """Member distances n + pad: 16-byte aligned members take the float4
-    path, the others the staged one; both must agree with the oracle."""
+def test_fused_member_alignment(kind, n, pad):
+    """Member distances n + pad on both sides: 16-byte aligned members take
+    the float4 paths (DCT-II / DST-II input, DCT-III / DST-III output), the
+    others the staged ones; both must agree with the oracle."""
     import torch
 
     hm = 5
+    d = n + pad
     rng = np.random.default_rng(n + pad)
-    x = rng.uniform(-1, 1, span(hm, n + pad, n, 1)).astype(np.float32)
-    plan = plfft.make_plan("r2r", n, hm, 1, n + pad, 1, n, r2r_kind=plfft.R2RKind[kind])
+    x = rng.uniform(-1, 1, span(hm, d, n, 1)).astype(np.float32)
+    plan = plfft.make_plan("r2r", n, hm, 1, d, 1, d, r2r_kind=plfft.R2RKind[kind])
     assert "fused" in plan.describe(), plan.describe()
-    y = run_plan(plan, x, hm * n, torch.float32).reshape(hm, n)
-    ref = oracle.r2r(gather(x, hm, n + pad, n, 1).astype(np.float64), kind)
-    assert oracle.rel_l2(y, ref) <= oracle.fp32_tol(2 * n)
+    y = run_plan(plan, x, span(hm, d, n, 1), torch.float32)
+    ref = oracle.r2r(gather(x, hm, d, n, 1).astype(np.float64), kind)
+    assert oracle.rel_l2(gather(y, hm, d, n, 1), ref) <= oracle.fp32_tol(2 * n)
 
 
 @pytest.mark.parametrize("n", [1024, 4096])
