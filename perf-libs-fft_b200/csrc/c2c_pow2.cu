@@ -12,6 +12,8 @@
 // This is the fast path for the reference's power-of-two C2C plans
 // (src/planner/strategies/cooley_tukey.hpp:622-679 recursion of radix-r
 // twiddle levels; here all levels of one transform stay on chip).
+#include <cstdlib>
+
 #include "kernels.h"
 #include "ptx.cuh"
 #include "pow2_stages.cuh"
@@ -160,6 +162,11 @@ __global__ void __launch_bounds__(pow2_max_threads<E>(), pow2_min_blocks<E>()) c
     mbar_fence_init();
   }
   __syncthreads();
+  // launched programmatically: the set-up above overlaps the end of the
+  // previous launch; no global input is read and no output written before
+  // that launch has completed
+  griddep_wait();
+  griddep_launch_dependents();
   // with direct stores a slot is free again right after its transform, so
   // all R slots hold loads in flight; with bulk stores one slot drains
   const int ahead = L.dstore ? R : R - 1;
@@ -394,8 +401,21 @@ static cudaError_t run_pow2(const Pow2Launch& L, cudaStream_t st) {
     const int64_t cap = int64_t(per_sm) * sm_count();
     const int64_t per_cta = (ngroups + cap - 1) / cap;
     const int64_t grid = (ngroups + per_cta - 1) / per_cta;
-    k<<<dim3(unsigned(grid)), dim3(threads), smem, st>>>(L);
-    return cudaGetLastError();
+    // programmatic dependent launch: the CTAs of this launch may be placed
+    // while the previous launch in the stream drains (the kernel waits for
+    // it before touching global data)
+    static const bool pdl = std::getenv("PLFFT_B200_NO_PDL") == nullptr;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(grid));
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = size_t(smem);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k, L);
   }
   const int smem = pow2_smem_bytes(N, L.g);
   {

@@ -83,6 +83,16 @@ __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// programmatic dependent launch: griddep_wait blocks until the grids this
+// launch depends on have completed and their writes are visible (it returns
+// at once when there are none); griddep_launch_dependents lets the next
+// launch in the stream, if it was launched programmatically, place its
+// CTAs on SMs as this grid's CTAs exit
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // asynchronous global -> shared copies (no register round trip), many in
 // flight per thread; completion by cp_async_wait_all + a barrier
 __device__ __forceinline__ void cp_async8(void* dst_smem, const void* src) {
