@@ -12,9 +12,8 @@
 // This is the fast path for the reference's power-of-two C2C plans
 // (src/planner/strategies/cooley_tukey.hpp:622-679 recursion of radix-r
 // twiddle levels; here all levels of one transform stay on chip).
-#include <cstdlib>
-
 #include "kernels.h"
+#include "launch_pdl.cuh"
 #include "ptx.cuh"
 #include "pow2_stages.cuh"
 
@@ -162,9 +161,9 @@ __global__ void __launch_bounds__(pow2_max_threads<E>(), pow2_min_blocks<E>()) c
     mbar_fence_init();
   }
   __syncthreads();
-  // launched programmatically: the set-up above overlaps the end of the
-  // previous launch; no global input is read and no output written before
-  // that launch has completed
+  // launched programmatically (launch_pdl.cuh): the set-up above overlaps
+  // the end of the previous launch; no global input is read and no output
+  // written before that launch has completed
   griddep_wait();
   griddep_launch_dependents();
   // with direct stores a slot is free again right after its transform, so
@@ -401,21 +400,7 @@ static cudaError_t run_pow2(const Pow2Launch& L, cudaStream_t st) {
     const int64_t cap = int64_t(per_sm) * sm_count();
     const int64_t per_cta = (ngroups + cap - 1) / cap;
     const int64_t grid = (ngroups + per_cta - 1) / per_cta;
-    // programmatic dependent launch: the CTAs of this launch may be placed
-    // while the previous launch in the stream drains (the kernel waits for
-    // it before touching global data)
-    static const bool pdl = std::getenv("PLFFT_B200_NO_PDL") == nullptr;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(unsigned(grid));
-    cfg.blockDim = dim3(threads);
-    cfg.dynamicSmemBytes = size_t(smem);
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = pdl ? 1 : 0;
-    return cudaLaunchKernelEx(&cfg, k, L);
+    return launch_pdl(k, dim3(unsigned(grid)), dim3(threads), size_t(smem), st, L);
   }
   const int smem = pow2_smem_bytes(N, L.g);
   {

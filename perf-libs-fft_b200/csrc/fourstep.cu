@@ -13,6 +13,7 @@
 // group of T = nl/E threads in registers, and the tile is stored walking the
 // contiguous dimension of the output.
 #include "kernels.h"
+#include "launch_pdl.cuh"
 #include "pow2_stages.cuh"
 #include "ptx.cuh"
 
@@ -27,6 +28,8 @@ __device__ __forceinline__ float2 fs_two_level(const TwoLevel& p, uint32_t e, in
 
 template <int NL, int E, int DIR>
 __global__ void __launch_bounds__(512) fourstep_pass_kernel(const FourStepLaunch L) {
+  griddep_wait();  // launched programmatically (launch_pdl.cuh)
+  griddep_launch_dependents();
   using P = P2<NL, E>;
   constexpr int T = P::T;
   constexpr int PITCH = (spad_len_c(NL) + 1) & ~1;
@@ -135,8 +138,8 @@ static cudaError_t run_fourstep(const FourStepLaunch& L, cudaStream_t st) {
     if (e != cudaSuccess) return e;
   }
   const int64_t blocks = (L.count + L.c - 1) / L.c;
-  fourstep_pass_kernel<NL, E, DIR><<<dim3(unsigned(blocks)), dim3((NL / E) * L.c), smem, st>>>(L);
-  return cudaGetLastError();
+  return launch_pdl(fourstep_pass_kernel<NL, E, DIR>, dim3(unsigned(blocks)), dim3((NL / E) * L.c), size_t(smem),
+                    st, L);
 }
 
 cudaError_t launch_fourstep_pass(int nl, int dir, const FourStepLaunch& L, cudaStream_t st) {

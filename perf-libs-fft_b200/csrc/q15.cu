@@ -25,6 +25,7 @@
 #include <stdint.h>
 
 #include "kernels.h"
+#include "launch_pdl.cuh"
 #include "ptx.cuh"
 
 namespace plfft_b200 {
@@ -185,6 +186,8 @@ __device__ __forceinline__ int pack(qc v) {
 // n <= 16: one thread per member
 template <int N, int DIR>
 __global__ void __launch_bounds__(256) q15_small_kernel(const Q15Launch L) {
+  griddep_wait();  // launched programmatically (launch_pdl.cuh)
+  griddep_launch_dependents();
   const int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (b >= L.howmany) return;
   constexpr int S = ilog2_c(N);
@@ -209,6 +212,8 @@ __host__ __device__ constexpr int q15_pitch(int n) { return ((17 * (n / 16) + 15
 // n = 16 m, m = 2..16: G = blockDim / 16 members per CTA
 template <int N, int DIR>
 __global__ void __launch_bounds__(256) q15_two_stage_kernel(const Q15Launch L) {
+  griddep_wait();  // launched programmatically (launch_pdl.cuh)
+  griddep_launch_dependents();
   constexpr int M = N / 16, SM = ilog2_c(M);
   constexpr int PITCH = q15_pitch(N);
   extern __shared__ int qsm[];
@@ -276,14 +281,13 @@ template <int N, int DIR>
 static cudaError_t run_q15(const Q15Launch& L, cudaStream_t st) {
   if constexpr (N <= 16) {
     const int64_t blocks = (L.howmany + 255) / 256;
-    q15_small_kernel<N, DIR><<<dim3(unsigned(blocks)), dim3(256), 0, st>>>(L);
+    return launch_pdl(q15_small_kernel<N, DIR>, dim3(unsigned(blocks)), dim3(256), 0, st, L);
   } else {
     constexpr int kThreads = 256, G = kThreads / 16;
     const int smem = q15_smem_bytes(N, G);
     const int64_t blocks = (L.howmany + G - 1) / G;
-    q15_two_stage_kernel<N, DIR><<<dim3(unsigned(blocks)), dim3(kThreads), smem, st>>>(L);
+    return launch_pdl(q15_two_stage_kernel<N, DIR>, dim3(unsigned(blocks)), dim3(kThreads), size_t(smem), st, L);
   }
-  return cudaGetLastError();
 }
 
 cudaError_t launch_q15(int n, int dir, const Q15Launch& L, cudaStream_t st) {

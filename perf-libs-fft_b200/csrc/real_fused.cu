@@ -28,7 +28,9 @@
 // DCT-II / DST-II pre/post passes (src/r2r_buffer_helper.hpp:316-335,
 // :455-469, :686-701, :828-854) folded into the on-chip FFT.
 #include "kernels.h"
+#include "launch_pdl.cuh"
 #include "pow2_stages.cuh"
+#include "ptx.cuh"
 
 namespace plfft_b200 {
 
@@ -139,6 +141,8 @@ __device__ __forceinline__ void finish_real(float2 (&v)[E], const RealFusedLaunc
 
 template <int M, int E, int KIND>
 __global__ void __launch_bounds__(pow2_max_threads<E>()) real_fused_kernel(const RealFusedLaunch L) {
+  griddep_wait();  // launched programmatically (launch_pdl.cuh)
+  griddep_launch_dependents();
   using P = P2<M, E>;
   constexpr int T = P::T;
   constexpr int N = 2 * M;
@@ -313,8 +317,7 @@ static cudaError_t run_real_fused(const RealFusedLaunch& L, cudaStream_t st) {
     if (e != cudaSuccess) return e;
   }
   const int64_t blocks = (L.howmany + L.g - 1) / L.g;
-  real_fused_kernel<M, E, KIND><<<dim3(unsigned(blocks)), dim3(T * L.g), smem, st>>>(L);
-  return cudaGetLastError();
+  return launch_pdl(real_fused_kernel<M, E, KIND>, dim3(unsigned(blocks)), dim3(T * L.g), size_t(smem), st, L);
 }
 
 template <int M, int E>
