@@ -426,7 +426,7 @@ def make_workload(name):
                                                          "R2C + C2R(1/N) FP32 round trip N=4096 batch=8192",
                                                          4096, 8192, profile="real_fused_n4096_b8192"),
         "dct2_n1024_b4096": lambda: PlanWorkload("dct2_n1024_b4096", "R2R DCT-II FP32 N=1024 batch=4096", "r2r",
-                                                 1024, 4096, r2r="DCT_2"),
+                                                 1024, 4096, r2r="DCT_2", profile="real_fused_dct2_n1024_b4096"),
         "dst2_n1024_b4096": lambda: PlanWorkload("dst2_n1024_b4096", "R2R DST-II FP32 N=1024 batch=4096", "r2r",
                                                  1024, 4096, r2r="DST_2"),
         "c2c_n1m_b64": lambda: PlanWorkload("c2c_n1m_b64", "C2C FP32 N=2^20 batch=64", "c2c", 1 << 20, 64),
