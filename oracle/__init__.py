@@ -1,7 +1,7 @@
 """FP64 CPU oracle -- test infrastructure only.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
-leg import this package, and only as the checker of the CUDA path.  It wraps
+leg import this package, and only to check the CUDA path's results.  It wraps
 ``oracle/lib/liboracle.so`` (built from ``oracle/oracle.c`` by ``make -C
 oracle``), which restates the reference's transform definitions
 (arm/perf-libs-fft docs/plfft.md:100-212, include/plfft.h:98-134) as FP64

@@ -2,7 +2,7 @@
  * FP64 CPU oracle for the batched 1D transforms -- TEST INFRASTRUCTURE ONLY.
  *
  * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may
- * load this library, and only as the checker.  The product path
+ * load this library, and only to check results.  The product path
  * (libplfft_b200.so) never calls it.
  *
  * Conventions restated from the reference (arm/perf-libs-fft):
