@@ -21,6 +21,12 @@ the FP64 port of the reference's transform definitions in oracle/ (the
 reference itself is AArch64-only and does not build on an x86_64 host), on
 all host cores, as K steps of a calibrated sample of the same workload.
 
+The CPU-baseline leg runs the FP64 oracle on a sample of members taken from
+the last buffer set the timed loop transformed, and compares the device's
+outputs for those members with it: the line's `parity` field (worst member
+rel-L2 against the FP32 gate, or bit-exactness for Q0.15).  A failed check
+prints the line and exits with status 1.
+
 Multi-GPU (torchrun, one rank per GPU): every rank runs the full workload on
 its own GPU (batch replicas, weak scaling); there is no data-path collective.
 """
@@ -57,6 +63,10 @@ class Workload:
     def config(self):
         return {}
 
+    def extra(self, stream, steps):
+        """Additional keys for the JSON line (measured after the timed region)."""
+        return {}
+
 
 def _rand_complex(count, gen):
     import torch
@@ -64,6 +74,45 @@ def _rand_complex(count, gen):
     re_ = torch.rand(count, device="cuda", generator=gen) * 2 - 1
     im_ = torch.rand(count, device="cuda", generator=gen) * 2 - 1
     return torch.complex(re_, im_)
+
+
+def spread_members(howmany, m, seed=0):
+    """m member indices spread over the batch, always with the first and the
+    last few (the final partial group of the last CTAs)."""
+    import numpy as np
+
+    m = max(1, min(m, howmany))
+    tail = list(range(max(0, howmany - min(8, m // 2)), howmany))
+    rng = np.random.default_rng(seed)
+    rest = m - len(tail)
+    body = rng.choice(max(1, howmany - len(tail)), max(0, min(rest, howmany - len(tail))), replace=False)
+    return np.array(sorted(set(body.tolist()) | set(tail) | {0}))[:m] if m < howmany else np.arange(howmany)
+
+
+def _rows(t, idx, width, np_dtype):
+    """Members idx of a flat device buffer of contiguous rows, as a host array."""
+    import numpy as np
+    import torch
+
+    v = t.view(-1)
+    sel = torch.as_tensor(idx, device=v.device, dtype=torch.int64)
+    if np_dtype == np.complex64:
+        v = v.view(torch.complex64)
+    elif np_dtype == np.int16:
+        v = v.view(torch.int32)
+    out = v.view(-1, width).index_select(0, sel).cpu().numpy()
+    return out.view(np.int16).reshape(len(idx), width, 2) if np_dtype == np.int16 else out
+
+
+def _parity(got, ref, tol, what):
+    """Worst member rel-L2 of got against ref (rows), checked against tol."""
+    import numpy as np
+
+    num = np.linalg.norm(np.asarray(got, np.complex128) - ref, axis=-1)
+    den = np.maximum(np.linalg.norm(ref, axis=-1), 1e-300)
+    worst = float((num / den).max())
+    return {"members": int(got.shape[0]), "worst_member_rel_l2": worst, "tol": tol, "ok": bool(worst <= tol),
+            "against": what}
 
 
 class PlanWorkload(Workload):
@@ -74,6 +123,7 @@ class PlanWorkload(Workload):
         if kind != "c2c":
             self.data = "synthetic (seeded real U[-1,1))"
         self.r2r, self.precision, self.profile = r2r, precision, profile
+        self.last_set = None
 
     def sizes(self):
         n, b = self.n, self.batch
@@ -119,6 +169,7 @@ class PlanWorkload(Workload):
         self.launches = self.plan.launch_count()
 
     def step(self, i, stream):
+        self.last_set = i % self.sets
         self.plan.execute_async(self.ins[i % self.sets].data_ptr(), self.outs[i % self.sets].data_ptr(),
                                 self.ws.data_ptr(), stream)
 
@@ -141,31 +192,63 @@ class PlanWorkload(Workload):
     def describe(self):
         return self.plan.describe()
 
-    def cpu_sample(self, threads):
-        """FP64 oracle on a bounded sample; returns (run one sample, sample bytes, text)."""
+    def sample_count(self):
+        import numpy as np
+
+        # about 2e6 n log n of oracle work, and at least 4 members
+        m = max(4, min(self.batch, int(2e6 // max(1, self.n * max(1, np.log2(self.n))))))
+        if self.kind == "r2r" and self.r2r not in ("DCT_2", "DST_2"):
+            m = max(1, min(self.batch, int(4e7 // (self.n * self.n))))
+        elif self.kind == "r2r":
+            m = max(1, min(self.batch, int(2e6 // max(1, 2 * self.n * np.log2(2 * self.n)))))
+        return m
+
+    def device_rows(self, idx):
+        """(inputs, outputs) of members idx of the last timed buffer set."""
+        import numpy as np
+
+        k = self.last_set
+        n, h = self.n, self.n // 2 + 1
+        if self.kind == "c2c":
+            return _rows(self.ins[k], idx, n, np.complex64), _rows(self.outs[k], idx, n, np.complex64)
+        if self.kind == "r2c":
+            return _rows(self.ins[k], idx, n, np.float32), _rows(self.outs[k], idx, h, np.complex64)
+        if self.kind == "c2r":
+            return _rows(self.ins[k], idx, h, np.complex64), _rows(self.outs[k], idx, n, np.float32)
+        return _rows(self.ins[k], idx, n, np.float32), _rows(self.outs[k], idx, n, np.float32)
+
+    def cpu_sample(self, threads, from_device=False):
+        """FP64 oracle over a bounded sample of members.  Returns (run the
+        sample, sample bytes, text, check): with from_device the sample is the
+        members of the last timed set and check(result) compares the device's
+        outputs for them with the oracle's."""
         import numpy as np
 
         import oracle
 
-        per = self.n * 16
-        m = max(1, min(self.batch, int(2e6 // max(1, self.n * max(1, np.log2(self.n))))))
-        if self.kind == "r2r":
-            m = max(1, min(self.batch, int(4e7 // (self.n * self.n))))
+        m = self.sample_count()
+        idx = spread_members(self.batch, m)
+        m = len(idx)
         rng = np.random.default_rng(0)
-        if self.kind == "c2c":
+        y = None
+        if from_device:
+            x, y = self.device_rows(idx)
+            x = x.astype(np.complex128 if np.iscomplexobj(x) else np.float64)
+        elif self.kind == "c2c":
             x = rng.uniform(-1, 1, (m, self.n)) + 1j * rng.uniform(-1, 1, (m, self.n))
-            fn = lambda: oracle.c2c(x, -1, method="fft", threads=threads)  # noqa: E731
-        elif self.kind in ("r2c", "c2r"):
+        else:
             x = rng.uniform(-1, 1, (m, self.n))
-            fn = lambda: oracle.c2r(oracle.r2c(x, method="fft", threads=threads), self.n,  # noqa: E731
-                                    method="fft", threads=threads)
+        tol = 1e-6 if self.precision else oracle.fp32_tol(self.n)
+        if self.kind == "c2c":
+            fn = lambda: oracle.c2c(x, -1, method="fft", threads=threads)  # noqa: E731
+        elif self.kind == "r2c":
+            fn = lambda: oracle.r2c(x, method="fft", threads=threads)  # noqa: E731
         elif self.r2r in ("DCT_2", "DST_2"):
             # FP64 FFT of the length-2N even / odd extension, then the
             # post-rotation (the same mapping as the device path)
-            m = max(1, min(self.batch, int(2e6 // max(1, 2 * self.n * np.log2(2 * self.n)))))
-            x = rng.uniform(-1, 1, (m, self.n))
             k = np.arange(self.n)
             sign = 1.0 if self.r2r == "DCT_2" else -1.0
+            tol = oracle.fp32_tol(2 * self.n)
 
             def fn():
                 ext = np.concatenate([x, sign * x[:, ::-1]], axis=1).astype(np.complex128)
@@ -174,11 +257,14 @@ class PlanWorkload(Workload):
                     return (np.exp(-1j * np.pi * k / (2 * self.n)) * F[:, : self.n]).real
                 return -(np.exp(-1j * np.pi * (k + 1) / (2 * self.n)) * F[:, 1: self.n + 1]).imag
         else:
-            x = rng.uniform(-1, 1, (m, self.n))
+            tol = oracle.fp32_tol(2 * self.n)
             fn = lambda: oracle.r2r(x, self.r2r, threads=threads)  # noqa: E731
         frac = m / self.batch
         how = "direct sums" if (self.kind == "r2r" and self.r2r not in ("DCT_2", "DST_2")) else "mixed-radix FFT"
-        return fn, self.algo_bytes() * frac, f"{m} of {self.batch} transforms, FP64 {how} (oracle/)"
+        check = None
+        if y is not None:
+            check = lambda ref: _parity(y, ref, tol, "FP64 oracle (oracle/)")  # noqa: E731
+        return fn, self.algo_bytes() * frac, f"{m} of {self.batch} transforms, FP64 {how} (oracle/)", check
 
 
 class RoundTripWorkload(PlanWorkload):
@@ -220,6 +306,7 @@ class RoundTripWorkload(PlanWorkload):
 
     def step(self, i, stream):
         k = i % self.sets
+        self.last_set = k
         self.plan.execute_async(self.ins[k].data_ptr(), self.mid[k].data_ptr(), self.ws.data_ptr(), stream)
         self.inv.execute_async(self.mid[k].data_ptr(), self.outs[k].data_ptr(), self.ws.data_ptr(), stream)
 
@@ -248,23 +335,73 @@ class RoundTripWorkload(PlanWorkload):
     def describe(self):
         return self.plan.describe() + " + " + self.inv.describe()
 
+    def cpu_sample(self, threads, from_device=False):
+        import numpy as np
+
+        import oracle
+
+        n, h = self.n, self.n // 2 + 1
+        idx = spread_members(self.batch, self.sample_count())
+        m = len(idx)
+        if from_device:
+            k = self.last_set
+            x = _rows(self.ins[k], idx, n, np.float32).astype(np.float64)
+            spec = _rows(self.mid[k], idx, h, np.complex64)
+            back = _rows(self.outs[k], idx, n, np.float32)
+        else:
+            x = np.random.default_rng(0).uniform(-1, 1, (m, n))
+
+        def fn():
+            X = oracle.r2c(x, method="fft", threads=threads)
+            return X, oracle.c2r(X, n, method="fft", threads=threads) / n
+
+        check = None
+        if from_device:
+            def check(ref):
+                a = _parity(spec, ref[0], oracle.fp32_tol(n), "FP64 oracle (oracle/): R2C")
+                b = _parity(back, ref[1], oracle.fp32_tol(n), "FP64 oracle (oracle/): C2R(R2C)/N")
+                worst = a if a["worst_member_rel_l2"] >= b["worst_member_rel_l2"] else b
+                return dict(worst, ok=a["ok"] and b["ok"], against="FP64 oracle (oracle/): R2C and C2R(1/N)")
+        return (fn, self.algo_bytes() * m / self.batch,
+                f"{m} of {self.batch} transforms, FP64 R2C + C2R mixed-radix FFT (oracle/)", check)
+
 
 class GroupedWorkload(Workload):
-    name = "grouped_4000"
+    """The grouped mixed-length batch in one persistent launch per phase
+    (per_length=False), or the same transforms as one plain plan per
+    distinct length executed back to back (per_length=True)."""
+
     desc = ("grouped C2C FP32: 4000 transforms, log-uniform 16..65536 (60% pow2, 20% 2^a3^b5^c7^d, "
             "10% Rader primes, 10% Bluestein)")
     profile = None
 
-    def __init__(self, count=4000):
+    def __init__(self, count=4000, per_length=False):
         import numpy as np
 
         from helpers import grouped_lengths
 
         self.count = count
+        self.per_length = per_length
+        self.name = "grouped_4000_per_length" if per_length else "grouped_4000"
+        if per_length:
+            self.desc = self.desc.replace("in one", "") + "; one plain plan per distinct length"
         L = np.array(sorted(grouped_lengths(self.count, seed=2026)), np.int64)
         self.lengths = L
         self.offs = np.concatenate([[0], np.cumsum(L)[:-1]]).astype(np.int64)
         self.total = int(L.sum())
+        self.last_set = None
+
+    def _make_per_length(self):
+        """One plan per distinct length over the contiguous members of that length."""
+        import numpy as np
+
+        import plfft
+
+        plans = []
+        uniq, first, cnt = np.unique(self.lengths, return_index=True, return_counts=True)
+        for n, f, c in zip(uniq, first, cnt):
+            plans.append((plfft.make_plan("c2c", int(n), int(c)), int(self.offs[f]) * 8))
+        return plans
 
     def setup(self, gen):
         import torch
@@ -272,11 +409,17 @@ class GroupedWorkload(Workload):
         import plfft
 
         L = self.lengths
-        self.group = plfft.Group(L, self.offs, self.offs, plfft.FORWARD)
         self.sets = max(2, -(-4 * L2_BYTES // (16 * self.total)))
         self.ins = [_rand_complex(self.total, gen) for _ in range(self.sets)]
         self.outs = [torch.empty(self.total, dtype=torch.complex64, device="cuda") for _ in range(self.sets)]
-        self.launches = self.group.launch_count()
+        if self.per_length:
+            self.plans = self._make_per_length()
+            self.ws = torch.empty(max(1, max(p.workspace_size() for p, _ in self.plans)), dtype=torch.uint8,
+                                  device="cuda")
+            self.launches = sum(p.launch_count() for p, _ in self.plans)
+        else:
+            self.group = plfft.Group(L, self.offs, self.offs, plfft.FORWARD)
+            self.launches = self.group.launch_count()
 
     def algo_bytes(self):
         return 16 * self.total
@@ -292,9 +435,47 @@ class GroupedWorkload(Workload):
         return {"workload": self.desc, "count": self.count, "distinct_lengths": int(len(np.unique(self.lengths))),
                 "total_elements": self.total, "layout": "transforms contiguous, sorted by length"}
 
+    def _run_per_length(self, k, stream):
+        xi, yo, ws = self.ins[k].data_ptr(), self.outs[k].data_ptr(), self.ws.data_ptr()
+        for p, off in self.plans:
+            p.execute_async(xi + off, yo + off, ws, stream)
+
     def step(self, i, stream):
         k = i % self.sets
-        self.group.execute_async(self.ins[k].data_ptr(), self.outs[k].data_ptr(), stream)
+        self.last_set = k
+        if self.per_length:
+            self._run_per_length(k, stream)
+        else:
+            self.group.execute_async(self.ins[k].data_ptr(), self.outs[k].data_ptr(), stream)
+
+    def extra(self, stream, steps):
+        """Grouped line: the same transforms as per-length plain plans on the
+        same buffers, timed the same way, and the grouped launch's speed-up."""
+        if self.per_length:
+            return {}
+        import torch
+
+        self.plans = self._make_per_length()
+        self.ws = torch.empty(max(1, max(p.workspace_size() for p, _ in self.plans)), dtype=torch.uint8,
+                              device="cuda")
+        sh = stream.cuda_stream
+        for i in range(3):
+            self._run_per_length(i % self.sets, sh)
+        torch.cuda.synchronize()
+        reps = max(3, min(steps, 20))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(reps):
+            self._run_per_length(i % self.sets, sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        per_ms = e0.elapsed_time(e1) / reps
+        launches = sum(p.launch_count() for p, _ in self.plans)
+        del self.plans
+        return {"per_length": {"ms_per_step": per_ms, "value": self.algo_bytes() / (per_ms * 1e-3) / 1e9,
+                               "unit": "GB/s", "plans": int(len(set(self.lengths.tolist()))),
+                               "launches_per_step": launches},
+                "_per_length_ms": per_ms}
 
     def e2e(self, steps):
         import torch
@@ -305,7 +486,10 @@ class GroupedWorkload(Workload):
 
         def one():
             self.ins[0].copy_(hx, non_blocking=True)
-            self.group.execute_async(self.ins[0].data_ptr(), self.outs[0].data_ptr(), s.cuda_stream)
+            if self.per_length:
+                self._run_per_length(0, s.cuda_stream)
+            else:
+                self.group.execute_async(self.ins[0].data_ptr(), self.outs[0].data_ptr(), s.cuda_stream)
             hy.copy_(self.outs[0], non_blocking=True)
 
         one()
@@ -316,29 +500,51 @@ class GroupedWorkload(Workload):
             one()
         e1.record(s)
         torch.cuda.synchronize()
-        return (e0.elapsed_time(e1) / steps, 8 * self.total, 8 * self.total,
-                "H2D + plfft_cuda_group_execute_async + D2H (pinned)")
+        api = "H2D + " + ("plfft_plan_execute_async per length" if self.per_length
+                          else "plfft_cuda_group_execute_async") + " + D2H (pinned)"
+        return e0.elapsed_time(e1) / steps, 8 * self.total, 8 * self.total, api
 
     def describe(self):
+        if self.per_length:
+            return f"{len(self.plans)} per-length plans"
         return self.group.describe()
 
-    def cpu_sample(self, threads):
+    def cpu_sample(self, threads, from_device=False):
         import numpy as np
 
         import oracle
 
-        pick = self.lengths[:: max(1, len(self.lengths) // 200)]
-        xs = [np.random.default_rng(int(n)).standard_normal(n) + 0j for n in pick]
+        sel = np.arange(0, len(self.lengths), max(1, len(self.lengths) // 200))
+        sel = np.union1d(sel, [len(self.lengths) - 1])
+        pick = self.lengths[sel]
+        if from_device:
+            xin = self.ins[self.last_set]
+            yout = self.outs[self.last_set]
+            xs = [xin[int(o):int(o) + int(n)].cpu().numpy().astype(np.complex128)
+                  for o, n in zip(self.offs[sel], pick)]
+            ys = [yout[int(o):int(o) + int(n)].cpu().numpy() for o, n in zip(self.offs[sel], pick)]
+        else:
+            xs = [np.random.default_rng(int(n)).standard_normal(n) + 0j for n in pick]
 
         def fn():
-            for x in xs:
-                oracle.c2c(x[None], -1, method="fft", threads=threads)
-        return fn, 16 * float(np.sum(pick)), f"{len(pick)} of {self.count} transforms, FP64 FFT (oracle/)"
+            return [oracle.c2c(x[None], -1, method="fft", threads=threads)[0] for x in xs]
+
+        check = None
+        if from_device:
+            def check(refs):
+                ratios = []
+                for y, r, n in zip(ys, refs, pick):
+                    ratios.append(oracle.rel_l2(y, r) / oracle.fp32_tol(int(n)))
+                worst = float(max(ratios))
+                return {"members": len(ys), "worst_rel_l2_over_tol": worst, "tol": "4*log2(N)*2^-24 per length",
+                        "ok": bool(worst <= 1.0), "against": "FP64 oracle (oracle/)"}
+        return fn, 16 * float(np.sum(pick)), f"{len(pick)} of {self.count} transforms, FP64 FFT (oracle/)", check
 
 
 class AdjointWorkload(PlanWorkload):
     """Differentiation step: R2C forward + adjoint (C2R with Hermitian-fold
-    weights) of the weighted power loss, x FP32 1024 x 8192."""
+    weights) of the weighted power loss, x FP32 1024 x 8192.  The adjoint
+    writes a gradient buffer of its own, so the inputs stay the seeded data."""
 
     def __init__(self):
         super().__init__("diff_r2c_n8192_b1024", "loss = sum W |R2C(x)|^2 forward + adjoint, N=8192 batch=1024",
@@ -350,12 +556,53 @@ class AdjointWorkload(PlanWorkload):
 
     def step(self, i, stream):
         k = i % self.sets
+        self.last_set = k
         self.plan.execute_async(self.ins[k].data_ptr(), self.outs[k].data_ptr(), self.ws.data_ptr(), stream)
-        self.plan.execute_adjoint(self.outs[k].data_ptr(), self.ins[(k + 1) % self.sets].data_ptr(), 0, stream)
+        self.plan.execute_adjoint(self.outs[k].data_ptr(), self.grads[k].data_ptr(), 0, stream)
 
     def setup(self, gen):
+        import torch
+
         super().setup(gen)
+        self.grads = [torch.empty_like(x) for x in self.ins]
         self.launches *= 2
+
+    def cpu_sample(self, threads, from_device=False):
+        import numpy as np
+
+        import oracle
+
+        n, h = self.n, self.n // 2 + 1
+        idx = spread_members(self.batch, self.sample_count())
+        m = len(idx)
+        if from_device:
+            k = self.last_set
+            x = _rows(self.ins[k], idx, n, np.float32).astype(np.float64)
+            spec = _rows(self.outs[k], idx, h, np.complex64)
+            grad = _rows(self.grads[k], idx, n, np.float32)
+        else:
+            x = np.random.default_rng(0).uniform(-1, 1, (m, n))
+        # adjoint of R2C under <a, b> = Re sum conj(a) b: x_j = Re sum_k g_k e^{+2 pi i jk/n}
+        # over the stored bins, i.e. C2R with the interior bins halved
+        wgt = np.full(h, 0.5)
+        wgt[0] = 1.0
+        if n % 2 == 0:
+            wgt[-1] = 1.0
+
+        def fn():
+            X = oracle.r2c(x, method="fft", threads=threads)
+            return X, oracle.c2r(X * wgt, n, method="fft", threads=threads)
+
+        check = None
+        if from_device:
+            def check(ref):
+                a = _parity(spec, ref[0], oracle.fp32_tol(n), "R2C")
+                b = _parity(grad, oracle.c2r(spec.astype(np.complex128) * wgt, n, method="fft", threads=threads),
+                            oracle.fp32_tol(n), "adjoint")
+                worst = a if a["worst_member_rel_l2"] >= b["worst_member_rel_l2"] else b
+                return dict(worst, ok=a["ok"] and b["ok"], against="FP64 oracle (oracle/): R2C and its adjoint")
+        return (fn, self.algo_bytes() * m / self.batch,
+                f"{m} of {self.batch} transforms, FP64 R2C + adjoint mixed-radix FFT (oracle/)", check)
 
 
 class Q15Workload(PlanWorkload):
@@ -406,16 +653,29 @@ class Q15Workload(PlanWorkload):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / steps, ib, ob, "plfft_plan_execute(host pinned buffers)"
 
-    def cpu_sample(self, threads):
+    def cpu_sample(self, threads, from_device=False):
         import numpy as np
 
         import oracle
 
-        m = min(self.batch, 4096)
-        rng = np.random.default_rng(0)
-        x = rng.integers(-(1 << 14), 1 << 14, (m, self.n, 2)).astype(np.int16)
+        idx = spread_members(self.batch, min(self.batch, 4096))
+        m = len(idx)
+        y = None
+        if from_device:
+            k = self.last_set
+            x = _rows(self.ins[k], idx, self.n, np.int16)
+            y = _rows(self.outs[k], idx, self.n, np.int16)
+        else:
+            rng = np.random.default_rng(0)
+            x = rng.integers(-(1 << 14), 1 << 14, (m, self.n, 2)).astype(np.int16)
+        check = None
+        if y is not None:
+            def check(ref):
+                bad = int(np.count_nonzero(np.any(y != ref, axis=(1, 2))))
+                return {"members": m, "mismatched_members": bad, "bit_exact": bad == 0, "ok": bad == 0,
+                        "against": "bit-exact Q0.15 restatement (oracle/q15.c)"}
         return (lambda: oracle.q15_c2c(x, -1), self.algo_bytes() * m / self.batch,
-                f"{m} of {self.batch} transforms, bit-exact Q0.15 C restatement (oracle/q15.c, 1 thread)")
+                f"{m} of {self.batch} transforms, bit-exact Q0.15 C restatement (oracle/q15.c, 1 thread)", check)
 
 
 def make_workload(name):
@@ -439,6 +699,7 @@ def make_workload(name):
                                                           "c2c", 1 << 16, 1024, precision=1,
                                                           profile="split_bf16_pass_n64k_b1024"),
         "grouped_4000": lambda: GroupedWorkload(),
+        "grouped_4000_per_length": lambda: GroupedWorkload(per_length=True),
         "q15_n256_b16384": lambda: Q15Workload("q15_n256_b16384", "C2C Q0.15 forward N=256 batch=16384", 256, 16384),
         "diff_r2c_n8192_b1024": lambda: AdjointWorkload(),
     }
@@ -447,6 +708,7 @@ def make_workload(name):
 
 WORKLOAD_NAMES = ["c2c_n1024_b4096", "r2c_c2r_n4096_b8192", "dct2_n1024_b4096", "dst2_n1024_b4096", "c2c_n1m_b64",
                   "c2c_n64k_b1024", "c2c_n1m_b64_split_bf16", "c2c_n64k_b1024_split_bf16", "grouped_4000",
+                  "grouped_4000_per_length",
                   "diff_r2c_n8192_b1024", "q15_n256_b16384"]
 
 
@@ -482,7 +744,15 @@ class ClockSampler:
     def __init__(self, gpu):
         self.gpu = gpu
         self.proc = None
-        self.lines = []
+        self.lines = []  # (host time, csv line)
+        self.t_mark = self.t_end = None
+
+    def mark(self):
+        """The timed region starts."""
+        self.t_mark = time.perf_counter()
+
+    def mark_end(self):
+        self.t_end = time.perf_counter()
 
     def start(self):
         try:
@@ -496,7 +766,7 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
 
     def stop(self):
         if self.proc is None:
@@ -509,7 +779,15 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        # samples inside the timed region (with one sampling period of slack);
+        # a region shorter than the period falls back to every sample taken
+        # while the workload ran (warm-up, timed loop, per-step timing)
+        lines = [ln for t, ln in self.lines
+                 if self.t_mark is not None and self.t_mark - 0.1 <= t <= (self.t_end or t) + 0.1]
+        window = "timed region"
+        if len(lines) < 2:
+            lines, window = [ln for _, ln in self.lines], "warm-up through per-step timing"
+        for ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -523,7 +801,8 @@ class ClockSampler:
                     reasons.add(nm)
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm),
+                "window": window}
 
 
 def _calibrate(fn):
@@ -534,29 +813,41 @@ def _calibrate(fn):
     return max(time.perf_counter() - t0, 1e-6)
 
 
-def cpu_baseline(w, target_s=10.0):
-    """The CPU oracle on repetitions of a bounded sample, about target_s seconds."""
+def cpu_baseline(w, target_s=10.0, from_device=True):
+    """The CPU oracle on repetitions of a bounded sample, about target_s
+    seconds.  The sample is members of the last timed buffer set; the
+    oracle's result for it is also the parity check of the device outputs."""
+    import platform
+
     import oracle
 
     threads = oracle.max_threads()
-    fn, sbytes, text = w.cpu_sample(threads)
-    reps = max(1, min(100000, int(target_s / _calibrate(fn))))
+    fn, sbytes, text, check = w.cpu_sample(threads, from_device=from_device)
+    ref = fn()
+    parity = check(ref) if check is not None else None
+    t0 = time.perf_counter()
+    fn()
+    one = max(time.perf_counter() - t0, 1e-6)
+    reps = max(1, min(100000, int(target_s / one)))
     t0 = time.perf_counter()
     for _ in range(reps):
         fn()
     dt = (time.perf_counter() - t0) / reps
     return {"value": sbytes / dt / 1e9, "unit": "GB/s", "cores": threads, "kind": "port",
-            "sample": f"{text}, {reps} repetitions ({reps * dt:.1f} s)"}
+            "host_arch": platform.machine(),
+            "sample": f"{text}, {reps} repetitions ({reps * dt:.1f} s)"}, parity
 
 
 def reference_arm(w, steps, warmup, budget_s=120.0):
     """The reference's CPU path (the oracle port: the reference cannot be
-    built here) timed as `steps` steps of a bounded sample after `warmup`
-    untimed ones; the whole run stays within about budget_s seconds."""
+    built on this host) timed as `steps` steps of a bounded sample after
+    `warmup` untimed ones; the whole run stays within about budget_s seconds."""
+    import platform
+
     import oracle
 
     threads = oracle.max_threads()
-    fn, sbytes, text = w.cpu_sample(threads)
+    fn, sbytes, text, _ = w.cpu_sample(threads)
     one = _calibrate(fn)
     per_step = min(10.0, max(0.05, budget_s / max(1, steps + warmup)))
     reps = max(1, int(per_step / one))
@@ -568,6 +859,7 @@ def reference_arm(w, steps, warmup, budget_s=120.0):
     dt = time.perf_counter() - t0
     value = steps * reps * sbytes / dt / 1e9
     return value, {"value": value, "unit": "GB/s", "cores": threads, "kind": "port",
+                   "host_arch": platform.machine(),
                    "sample": f"{text}, {reps} repetitions per step"}, dt * 1e3 / steps
 
 
@@ -629,6 +921,10 @@ def main():
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
 
+    # the clock sampler runs from before the warm-up, so starting it costs
+    # the timed region nothing
+    sampler = ClockSampler(local)
+    sampler.start()
     for i in range(args.warmup):
         w.step(i, sh)
     torch.cuda.synchronize()
@@ -649,16 +945,16 @@ def main():
         args.steps = steps[0]
     barrier()
     torch.cuda.synchronize()
-    sampler = ClockSampler(local)
-    sampler.start()
+    sampler.mark()
     ev0.record(stream)
     for i in range(args.steps):
         w.step(i, sh)
     ev1.record(stream)
     torch.cuda.synchronize()
-    clocks = sampler.stop()
+    sampler.mark_end()
     barrier()
     ms = ev0.elapsed_time(ev1)
+    last_timed_set = getattr(w, "last_set", None)
     # per-step device time (each step bracketed by events)
     nk = min(args.steps, 50)
     kev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * nk)]
@@ -668,6 +964,9 @@ def main():
         kev[2 * i + 1].record(stream)
     torch.cuda.synchronize()
     step_ms = statistics.median(kev[2 * i].elapsed_time(kev[2 * i + 1]) for i in range(nk))
+    clocks = sampler.stop()
+    extra = w.extra(stream, args.steps)
+    per_length_ms = extra.pop("_per_length_ms", None)
     e2e = None
     if not args.no_e2e:
         e2e_ms, hb, db, api = w.e2e(max(3, min(args.steps, 20)))
@@ -690,9 +989,14 @@ def main():
     # several: the median event-bracketed step (all of the step's kernels)
     kernel_ms = ms_per_step if w.launches == 1 else step_ms
     achieved = abytes / (kernel_ms * 1e-3) / 1e9
-    cpu = None
+    cpu, parity = None, None
     if rank == 0 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(w)
+        # the per-step timing loop above ran steps 0..nk-1 last: redo the
+        # final timed step so the checked buffer set is the timed one's
+        if last_timed_set is not None:
+            w.step(args.steps - 1, sh)
+            torch.cuda.synchronize()
+        cpu, parity = cpu_baseline(w)
     if rank == 0:
         line = {
             "metric": f"{w.name} GB/s (algorithmic bytes)", "value": value, "unit": "GB/s",
@@ -711,10 +1015,17 @@ def main():
             "plan": w.describe(),
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "parity": parity,
         }
-        print(json.dumps(line))
+        line.update(extra)
+        if per_length_ms is not None:
+            line["speedup_vs_per_length"] = per_length_ms / ms_per_step
+        print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+    if parity is not None and not parity["ok"]:
+        print(f"bench: parity check failed: {parity}", file=sys.stderr)
+        sys.exit(1)
 
 
 if __name__ == "__main__":

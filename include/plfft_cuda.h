@@ -60,6 +60,18 @@ plfft_status_t plfft_cuda_execute_async(const plfft_plan_t *plan,
                                         const void *d_input, void *d_output,
                                         void *d_workspace, void *stream);
 
+/* Device-side failures of earlier stream-ordered executions of this plan.
+ * Waits for `stream` to drain, then reports PLFFT_DEVICE_TIMEOUT if any
+ * kernel of the plan (or of its adjoint) gave up a bounded wait since the
+ * last query -- the members that kernel owned are then unwritten -- and
+ * PLFFT_OK otherwise; the report is cleared.  The error convention of
+ * plfft_plan_execute (reference include/plfft.h:505-532: void, no checks)
+ * leaves no room for it, so the synchronous path reports the same status
+ * through plfft_cuda_get_last_status().  Status code from the reference's
+ * enum extension PLFFT_DEVICE_TIMEOUT (include/plfft.h of this library). */
+plfft_status_t plfft_cuda_plan_get_device_status(const plfft_plan_t *plan,
+                                                 void *stream);
+
 /* Adjoint (transpose for real data, conjugate transpose for complex data) of
  * the plan's transform, with the plan's scale: d_input uses the plan's OUTPUT
  * layout and d_output its INPUT layout.  No counterpart in the reference;

@@ -238,6 +238,15 @@ plfft_status_t plfft_cuda_execute_async(const plfft_plan_t* plan, const void* in
   return g_last_status;
 }
 
+plfft_status_t plfft_cuda_plan_get_device_status(const plfft_plan_t* plan, void* stream) {
+  if (!plan) return PLFFT_NULL_ARGUMENT;
+  const PlanData& p = plan->p;
+  if (cudaStreamSynchronize(static_cast<cudaStream_t>(stream)) != cudaSuccess) return PLFFT_CUDA_ERROR;
+  const plfft_status_t a = take_device_status(p.root.get());
+  const plfft_status_t b = take_device_status(p.adjoint.get());
+  return a != PLFFT_OK ? a : b;
+}
+
 // builds the adjoint schedule once (plan mutex); returns false on failure
 static bool ensure_adjoint(const PlanData& p) {
   std::lock_guard<std::mutex> lock(p.mu);

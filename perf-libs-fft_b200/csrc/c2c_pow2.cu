@@ -56,13 +56,19 @@ __global__ void __launch_bounds__(pow2_max_threads<E>(), pow2_min_blocks<E>()) c
       mbar_fence_init();
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    const bool stall = int(blockIdx.x) == L.stall_cta;  // test hook: no loads
+    if (threadIdx.x == 0 && !stall) {
       mbar_arrive_expect_tx(&bar, uint32_t(cnt) * N * 8u);
       for (int c = 0; c < cnt; ++c) bulk_g2s(inbuf + c * PITCH, L.in + (b0 + c) * L.idist, N * 8u, &bar);
     }
-    const bool ok = mbar_wait_bounded(&bar, 0);
+    const uint64_t lim = L.wait_ns ? L.wait_ns : kWaitLimitNs;
+    const bool ok = mbar_wait_bounded(&bar, 0, lim);
     if (__syncthreads_or(!ok)) {
-      if (threadIdx.x == 0) atomicExch(L.err, 1);
+      if (threadIdx.x == 0) {
+        report_device_error(L.err, 1);
+        // copies issued into this CTA's shared memory land before it exits
+        if (!stall) mbar_wait_bounded(&bar, 0, lim);
+      }
       return;
     }
     if (live) {
@@ -140,10 +146,14 @@ __global__ void __launch_bounds__(pow2_max_threads<E>(), pow2_min_blocks<E>()) c
     return r < G ? int(r) : G;
   };
   auto slot = [&](int k) { return ring + (k % R) * G * PITCH; };
+  const bool stall = int(blockIdx.x) == L.stall_cta;  // test hook: no loads
+  const uint64_t lim = L.wait_ns ? L.wait_ns : kWaitLimitNs;
+  uint32_t pending = 0;  // thread 0: slots with a load in flight
   auto issue = [&](int k) {  // thread 0 only
     const int64_t g = group_of(k);
-    if (g >= ngroups) return;
+    if (g >= ngroups || stall) return;
     const int cnt = count_of(g);
+    pending |= 1u << (k % R);
     uint64_t* b = &bar[k % R];
     mbar_arrive_expect_tx(b, uint32_t(cnt) * N * 8u);
     float2* dst = slot(k);
@@ -180,11 +190,18 @@ __global__ void __launch_bounds__(pow2_max_threads<E>(), pow2_min_blocks<E>()) c
     const int cnt = count_of(g);
     const bool live = grp < cnt;
     float2* mine = slot(k) + grp * PITCH;
-    const bool ok = mbar_wait_bounded(&bar[k % R], uint32_t(k / R) & 1u);
+    const bool ok = mbar_wait_bounded(&bar[k % R], uint32_t(k / R) & 1u, lim);
     if (__syncthreads_or(!ok)) {
-      if (threadIdx.x == 0) atomicExch(L.err, 1);
+      if (threadIdx.x == 0) {
+        report_device_error(L.err, 1);
+        // the load in flight in each slot belongs to the one group
+        // j in [k, k + R) with j % R == slot: let them land before exiting
+        for (int j = k; j < k + R; ++j)
+          if (pending & (1u << (j % R))) mbar_wait_bounded(&bar[j % R], uint32_t(j / R) & 1u, lim);
+      }
       break;
     }
+    if (threadIdx.x == 0) pending &= ~(1u << (k % R));
     float2 v[E];
     if (live) {
 #pragma unroll
@@ -261,6 +278,8 @@ __global__ void __launch_bounds__(512, 1) c2c_pow2_group_kernel(const Pow2Launch
   const int64_t lo = L.howmany * blockIdx.x / gridDim.x;
   const int64_t hi = L.howmany * (blockIdx.x + 1) / gridDim.x;
   const bool producer = (t == 0);
+  const uint64_t lim = L.wait_ns ? L.wait_ns : kWaitLimitNs;
+  uint32_t pending = 0;  // producer: slots with a load in flight
 
   auto gsync = [&]() {
     if constexpr (W == 1)
@@ -275,6 +294,7 @@ __global__ void __launch_bounds__(512, 1) c2c_pow2_group_kernel(const Pow2Launch
     meta[grp][s] = b;
     uint64_t* br = &bar[grp][s];
     if (b < hi) {
+      pending |= 1u << s;
       mbar_arrive_expect_tx(br, N * 8u);
       bulk_g2s(myslots + s * PITCH, L.in + b * L.idist, N * 8u, br);
     } else {
@@ -296,7 +316,7 @@ __global__ void __launch_bounds__(512, 1) c2c_pow2_group_kernel(const Pow2Launch
 
   for (int k = 0;; ++k) {
     const int s = k % NS;
-    const bool ok = mbar_wait_bounded(&bar[grp][s], uint32_t(k / NS) & 1u);
+    const bool ok = mbar_wait_bounded(&bar[grp][s], uint32_t(k / NS) & 1u, lim);
     bool failed;
     if constexpr (W == 1) {
       failed = __any_sync(0xffffffffu, !ok);
@@ -313,9 +333,15 @@ __global__ void __launch_bounds__(512, 1) c2c_pow2_group_kernel(const Pow2Launch
       failed = any != 0;
     }
     if (failed) {
-      if (producer) atomicExch(L.err, 1);
+      if (producer) {
+        report_device_error(L.err, 1);
+        // loads in flight belong to iterations j in [k, k + NS), one per slot
+        for (int j = k; j < k + NS; ++j)
+          if (pending & (1u << (j % NS))) mbar_wait_bounded(&bar[grp][j % NS], uint32_t(j / NS) & 1u, lim);
+      }
       break;  // group-local exit; other groups are independent
     }
+    if (producer) pending &= ~(1u << s);
     const int64_t b = meta[grp][s];
     if (b >= hi) break;
     float2* mine = myslots + s * PITCH;

@@ -71,7 +71,9 @@ struct Pow2Launch {
   int tws;    // CTA ring: stage twiddles copied to shared memory
   int dstore; // CTA ring: results stored from registers (no bulk store)
   int gp;    // warp-group kernel: groups per CTA (0 = as many as fit)  // persistent ring-buffered variant
-  int* err;  // set to 1 if a bounded device wait ran out
+  int* err;  // host-mapped status word: set to 1 if a bounded device wait ran out
+  uint64_t wait_ns;  // limit of each bounded wait (0: kWaitLimitNs)
+  int stall_cta;     // test hook: this CTA issues no loads, so its first wait runs out (-1: none)
 };
 
 // Real-data transforms through a complex DFT of length `len`

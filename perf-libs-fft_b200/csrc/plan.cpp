@@ -1,9 +1,9 @@
 // Planner: radix factorization, device twiddle tables and C2C schedules.
 #include "plan.hpp"
 
-#include <cstring>
-
 #include <algorithm>
+#include <atomic>
+#include <cstring>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -182,9 +182,15 @@ struct Pow2Params {
 struct C2CPow2Node : Node {
   Pow2Launch base{};
   int n = 0, e = 0, dir = -1;
-  DevBuf tw, err;
+  DevBuf tw;
+  HostWord status;
+  // test hook (PLFFT_B200_TEST_STALL_CTA): the CTA whose first load is
+  // withheld in the next run only
+  mutable std::atomic<int> stall_once{-1};
+  void status_words(std::vector<int*>& out) const override { out.push_back(status.p); }
   cudaError_t run(const void* in, void* out, void*, cudaStream_t st) const override {
     Pow2Launch L = base;
+    L.stall_cta = stall_once.exchange(-1);
     L.in = static_cast<const float2*>(in);
     L.out = static_cast<float2*>(out);
     const bool dist_in_ok = L.howmany == 1 || (L.idist % 2) == 0;
@@ -232,8 +238,7 @@ static std::unique_ptr<Node> make_pow2(int64_t n, const Layout& lay, int dir, fl
   for (int i = 0; i < ke; ++i) radices.push_back(e);
   std::vector<float2> tw;
   make_desc(int(n), radices, tw);
-  if (node->tw.upload(tw) != cudaSuccess || node->err.alloc(sizeof(int)) != cudaSuccess ||
-      cudaMemset(node->err.p, 0, sizeof(int)) != cudaSuccess) {
+  if (node->tw.upload(tw) != cudaSuccess || node->status.alloc() != cudaSuccess) {
     if (why) *why = "device allocation failed";
     return nullptr;
   }
@@ -248,7 +253,17 @@ static std::unique_ptr<Node> make_pow2(int64_t n, const Layout& lay, int dir, fl
   node->base.scale = scale;
   node->base.tw = node->tw.as<float2>();
   node->base.tw_len = int(tw.size());
-  node->base.err = node->err.as<int>();
+  node->base.err = node->status.device();
+  node->base.wait_ns = 0;
+  node->base.stall_cta = -1;
+  // Test hook for the device-timeout path: PLFFT_B200_TEST_STALL_CTA=k makes
+  // CTA k of this plan's first run withhold its loads, so its bounded wait
+  // (PLFFT_B200_TEST_WAIT_US microseconds) runs out and the run reports
+  // PLFFT_DEVICE_TIMEOUT; nothing is in flight when that CTA leaves.
+  if (const char* v = std::getenv("PLFFT_B200_TEST_STALL_CTA")) {
+    node->stall_once = std::atoi(v);
+    node->base.wait_ns = uint64_t(std::max(1, env_int("PLFFT_B200_TEST_WAIT_US", 2000))) * 1000u;
+  }
   // CTA ring, one transform per CTA for n = 1024 (g = 32 / T), 3 slots:
   // measured best at batch 4096 (4.09 TB/s; deeper rings, twiddles in
   // shared memory, register stores and the warp-group rings were slower)
@@ -816,6 +831,20 @@ std::vector<std::unique_ptr<Node>> make_c2c_candidates(int64_t n, const Layout& 
     if (!dup) uniq.push_back(std::move(c));
   }
   return uniq;
+}
+
+plfft_status_t take_device_status(const Node* node) {
+  if (!node) return PLFFT_OK;
+  std::vector<int*> words;
+  node->status_words(words);
+  plfft_status_t st = PLFFT_OK;
+  for (int* w : words) {
+    if (w && *reinterpret_cast<volatile int*>(w) != 0) {
+      st = PLFFT_DEVICE_TIMEOUT;
+      *reinterpret_cast<volatile int*>(w) = 0;
+    }
+  }
+  return st;
 }
 
 PlanData::~PlanData() {

@@ -74,6 +74,38 @@ struct DevBuf {
   }
 };
 
+// One int of pinned host memory mapped into the device's address space: a
+// kernel writes a failure code there, the host reads it once the stream that
+// ran the kernel has drained (no copy on the success path).
+struct HostWord {
+  int* p = nullptr;
+  HostWord() = default;
+  HostWord(const HostWord&) = delete;
+  HostWord& operator=(const HostWord&) = delete;
+  ~HostWord() {
+    if (p) cudaFreeHost(p);
+  }
+  cudaError_t alloc() {
+    cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&p), sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return e;
+    }
+    *p = 0;
+    return cudaSuccess;
+  }
+  // the address kernels write through (the same address under unified
+  // virtual addressing)
+  int* device() const {
+    void* d = nullptr;
+    if (p && cudaHostGetDevicePointer(&d, p, 0) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return static_cast<int*>(d);
+  }
+};
+
 // Strided batch layout, in elements of the buffer's own type.
 struct Layout {
   int64_t howmany;
@@ -89,7 +121,14 @@ struct Node {
   virtual std::string describe() const = 0;
   // number of kernel launches per run (for launch accounting)
   virtual int launches() const { return 1; }
+  // host-mapped status words its kernels report device-side failures in
+  // (bounded waits that ran out); composite nodes add their parts' words
+  virtual void status_words(std::vector<int*>& out) const { (void)out; }
 };
+
+// Reads and clears the status words of a node whose kernels have completed:
+// PLFFT_DEVICE_TIMEOUT if any reported a failure, else PLFFT_OK.
+plfft_status_t take_device_status(const Node* node);
 
 // ---------------------------------------------------------------------------
 // factorization and stage tables

@@ -112,6 +112,10 @@ struct ConvNode : Node {
   int64_t chunk = 1;
   DevBuf chirp, spec, pin, pout;
   std::unique_ptr<Node> fwd, bwd;  // length-m C2C plans over `chunk` contiguous members, in place
+  void status_words(std::vector<int*>& out) const override {
+    fwd->status_words(out);
+    bwd->status_words(out);
+  }
 
   size_t work_bytes() const { return (size_t(chunk) * size_t(m) * sizeof(float2) + 255) & ~size_t(255); }
   size_t sum_bytes() const { return (size_t(chunk) * sizeof(float2) + 255) & ~size_t(255); }

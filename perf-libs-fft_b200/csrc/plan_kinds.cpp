@@ -116,6 +116,10 @@ static std::unique_ptr<Node> make_root(const ConfigData& c, const Layout& lay, b
 // FP32 schedule for that chunk, round the results back to binary16.
 struct HalfIoNode : Node {
   std::unique_ptr<Node> inner, inner_tail;  // FP32 schedules: full chunk, last chunk
+  void status_words(std::vector<int*>& out) const override {
+    inner->status_words(out);
+    if (inner_tail) inner_tail->status_words(out);
+  }
   Layout user{};
   int64_t chunk = 1, nin = 0, nout = 0;
   int icomps = 1, ocomps = 1;
@@ -317,7 +321,10 @@ plfft_status_t execute_sync(const PlanData& p, const void* in, void* out) {
       if (e == cudaSuccess) e = ensure(p.stage_out, obytes);
       if (e == cudaSuccess) e = execute_pipelined(p, in, out);
       if (cur != p.device) cudaSetDevice(cur);
-      return e == cudaSuccess ? PLFFT_OK : PLFFT_CUDA_ERROR;
+      if (e != cudaSuccess) return PLFFT_CUDA_ERROR;
+      const plfft_status_t a = take_device_status(p.pipe_node.get());
+      const plfft_status_t b = take_device_status(p.pipe_tail.get());
+      return a != PLFFT_OK ? a : b;
     }
   }
   if (!din) {
@@ -337,7 +344,9 @@ plfft_status_t execute_sync(const PlanData& p, const void* in, void* out) {
   const cudaError_t s = cudaStreamSynchronize(p.stream);
   if (e == cudaSuccess) e = s;
   if (cur != p.device) cudaSetDevice(cur);
-  return e == cudaSuccess ? PLFFT_OK : PLFFT_CUDA_ERROR;
+  if (e != cudaSuccess) return PLFFT_CUDA_ERROR;
+  // a bounded device wait that ran out leaves its members unwritten
+  return take_device_status(p.root.get());
 }
 
 }  // namespace plfft_b200

@@ -20,6 +20,7 @@ struct RealWrapNode : Node {
   int64_t chunk = 1;
   size_t cbytes() const { return fp64 ? sizeof(double2) : sizeof(float2); }
   std::unique_ptr<Node> inner;  // C2C of length len over `chunk` contiguous members, in place
+  void status_words(std::vector<int*>& out) const override { inner->status_words(out); }
   size_t inner_ws() const { return inner->workspace(); }
   size_t workspace() const override {
     const size_t work = size_t(chunk) * size_t(len) * cbytes();

@@ -44,12 +44,33 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Wait for a barrier phase with an iteration limit.  Returns false if the
-// limit ran out (the caller records an error and leaves).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t limit = 1u << 22) {
-  for (uint32_t it = 0; it < limit; ++it)
+// nanoseconds of the GPU's global timer
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Default limit of a bounded device wait: a bulk copy of a few KB that has
+// not landed after two seconds will not land.
+constexpr uint64_t kWaitLimitNs = 2000000000ull;
+
+// Wait for a barrier phase for at most limit_ns nanoseconds.  Returns false
+// if the limit ran out (the caller records an error and leaves).  The timer
+// is only read once the first probe has failed.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint64_t limit_ns = kWaitLimitNs) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (;;) {
     if (mbar_try_wait(bar, parity)) return true;
-  return false;
+    if (globaltimer_ns() - t0 > limit_ns) return false;
+  }
+}
+
+// record a device-side failure in the plan's status word (host-mapped
+// memory: the host reads it after the stream has drained)
+__device__ __forceinline__ void report_device_error(int* status, int code) {
+  if (status) *reinterpret_cast<volatile int*>(status) = code;
 }
 
 // global -> shared bulk copy, completion signalled on `bar` (bytes % 16 == 0,

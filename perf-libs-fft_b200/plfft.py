@@ -133,6 +133,7 @@ _SIGS = [
     ("plfft_cuda_plan_get_launch_count", _INT, [_P]),
     ("plfft_cuda_plan_describe", _INT, [_P, ctypes.c_char_p, ctypes.c_size_t]),
     ("plfft_cuda_execute_async", _INT, [_P, _P, _P, _P, _P]),
+    ("plfft_cuda_plan_get_device_status", _INT, [_P, _P]),
     ("plfft_cuda_c2c_execute_noalloc", _INT, [_P, _P, _I64, _I64, _INT, _P]),
     ("plfft_cuda_execute_adjoint_async", _INT, [_P, _P, _P, _P, _P]),
     ("plfft_cuda_plan_get_adjoint_workspace_size", _INT, [_P, ctypes.POINTER(ctypes.c_size_t)]),
@@ -278,6 +279,12 @@ class Plan:
                                             ctypes.c_void_p(int(workspace)) if workspace else None,
                                             ctypes.c_void_p(int(stream)) if stream else None)
         _check(st, "plfft_cuda_execute_async")
+
+    def device_status(self, stream=0):
+        """plfft_cuda_plan_get_device_status: drains `stream`, returns (and
+        clears) the Status of device-side failures of earlier executions."""
+        return Status(lib().plfft_cuda_plan_get_device_status(self.handle,
+                                                              ctypes.c_void_p(int(stream)) if stream else None))
 
     def execute_adjoint(self, inp, out, workspace=0, stream=0):
         """Adjoint of this plan's transform (input = plan's output layout)."""
