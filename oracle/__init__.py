@@ -127,37 +127,49 @@ def fp32_tol(n):
 
 
 # ---------------------------------------------------------------------------
-# Q0.15 fixed point (oracle/q15.c): bit-exact restatement, n power of two <= 256
+# fixed point (oracle/fixed.c): bit-exact restatement of the Q0.15 and Q0.7
+# paths, n a power of two <= 4096
 # ---------------------------------------------------------------------------
 _LIBQ = None
+FIXED_MAX_N = 4096
 
 
 def _libq():
     global _LIBQ
     if _LIBQ is None:
-        path = os.path.join(_HERE, "lib", "liboracle_q15.so")
+        path = os.path.join(_HERE, "lib", "liboracle_fixed.so")
         if not os.path.exists(path):
             raise RuntimeError(f"oracle library missing: {path} (run make -C oracle)")
         L = ctypes.CDLL(path)
         i64 = ctypes.c_int64
         dp = ctypes.c_void_p
-        L.oracle_q15_c2c.argtypes = [dp, dp, i64, i64, i64, i64, ctypes.c_int]
-        L.oracle_q15_c2c.restype = ctypes.c_int
+        for name in ("oracle_q15_c2c", "oracle_q7_c2c"):
+            getattr(L, name).argtypes = [dp, dp, i64, i64, i64, i64, ctypes.c_int]
+            getattr(L, name).restype = ctypes.c_int
         L.oracle_q15_twiddles.argtypes = [i64, ctypes.c_int, dp]
         L.oracle_q15_twiddles.restype = None
         _LIBQ = L
     return _LIBQ
 
 
-def q15_c2c(x, direction=-1):
-    """x: int16 [howmany, n, 2] (re, im) -> int16 [howmany, n, 2], scaled by 1/n."""
-    x = np.ascontiguousarray(x, dtype=np.int16)
+def _fixed_c2c(x, direction, dtype, fn):
+    x = np.ascontiguousarray(x, dtype=dtype)
     hm, n = x.shape[0], x.shape[1]
     y = np.empty_like(x)
-    rc = _libq().oracle_q15_c2c(_ptr(x), _ptr(y), n, hm, n, n, int(direction))
+    rc = fn(_ptr(x), _ptr(y), n, hm, n, n, int(direction))
     if rc != 0:
-        raise ValueError(f"q15 oracle: unsupported length {n}")
+        raise ValueError(f"fixed-point oracle: unsupported length {n}")
     return y
+
+
+def q15_c2c(x, direction=-1):
+    """x: int16 [howmany, n, 2] (re, im) -> int16 [howmany, n, 2], scaled by 1/n."""
+    return _fixed_c2c(x, direction, np.int16, _libq().oracle_q15_c2c)
+
+
+def q7_c2c(x, direction=-1):
+    """x: int8 [howmany, n, 2] (re, im) -> int8 [howmany, n, 2], scaled by 1/n."""
+    return _fixed_c2c(x, direction, np.int8, _libq().oracle_q7_c2c)
 
 
 def q15_twiddles(n, direction=-1):

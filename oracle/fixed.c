@@ -1,0 +1,386 @@
+/*
+ * Bit-exact CPU restatement of the reference's fixed-point C2C path, Q0.15
+ * and Q0.7 -- TEST INFRASTRUCTURE ONLY (same rules as oracle.c: only tests/
+ * and the CPU-baseline leg of bench.py load it, to check results).
+ *
+ * What is restated (arm/perf-libs-fft), for lanes of B = 16 or 8 bits:
+ *   Arithmetic semantics (src/providers/jit/print_algo.cpp:1228-1230,
+ *   src/providers/jit/emit.hpp:150-175 and :370-425, constant lowering
+ *   print_algo.cpp:2150-2290):
+ *     - every codelet input is pre-scaled by a rounding shift right by
+ *       log2(radix) (srshr), so a whole transform is scaled by 1/N;
+ *     - additions and subtractions saturate to B bits (sqadd / sqsub);
+ *     - a multiply by a real constant k (a Q0.(B-1) value) is
+ *       (a k + 2^(B-2)) >> (B-1), saturated: sqrdmulh for Q0.15, smull +
+ *       sqrshrn #7 for Q0.7 (the two agree on this formula); multiplying by
+ *       +-i swaps re/im and uses k = -2^(B-1) or 2^(B-1) - 1 on the lanes;
+ *     - a complex product with a twiddle (and the fused constant products
+ *       of the radix-8/16 codelets) is two B x B products accumulated in a
+ *       2B-bit lane (smull / smlal / smlsl, wrapping at 2B bits) and
+ *       narrowed once by a rounding, saturating shift by B - 1 (sqrshrn).
+ *   Codelets: radix 2, 4, 8 and the fixed-point split-radix 16
+ *   (src/providers/jit/split_radix_z16.cpp, selected for fixed point by
+ *   src/providers/jit/wfta_nfact.cpp:89-97); the backward codelet of
+ *   length r produces, at output k, the forward codelet's output r-k.
+ *   Composition: the reference's ESTIMATE plan (planner/planner.cpp:51-175,
+ *   first applicable strategy; base kernels {2, 4, 8, 16},
+ *   providers/aot/aot_kernel_data.cpp:296-300):
+ *     N <= 16        one codelet per member;
+ *     N = 16 m       (m <= 16) cooley_tukey_ab(16): length-m codelets down
+ *                    the 16 columns x[c + 16 q], then per row j a 16-point
+ *                    codelet whose inputs i >= 1 are multiplied by the
+ *                    twiddle W_N^{dir i j} (row 0 untwiddled), writing
+ *                    y[j + m k] (planner/strategies/cooley_tukey.hpp:82-143,
+ *                    622-680);
+ *     N = 256 m'     (m' = 2..16) cooley_tukey_ab(16) whose length-16 m'
+ *                    sub-transforms are cooley_tukey_ac(16)
+ *                    (cooley_tukey.hpp:331-385, 682-748): length-m' codelets
+ *                    down the 256 columns x[c + 256 q] into b1[c + 256 k];
+ *                    then for column t < 16 and row i0 < m' a 16-point
+ *                    codelet over b1[256 i0 + t + 16 i], inputs i >= 1 of
+ *                    rows i0 >= 1 twiddled by W_{16 m'}^{dir i i0}, into
+ *                    b0[16 i0 + t + 16 m' k]; then the twiddled 16-point
+ *                    rows of the N = 16 m case over b0.
+ *   Twiddles: cvt(x) = sat(trunc(float(x) * 2^(B-1))) of cos and sin of the
+ *   angle (src/generate_twiddles.hpp:72-132, src/plfft_convert.hpp:36-54),
+ *   stored as the premultiplied pairs (c, s), (-s, c).
+ *
+ * Parity pin: tests/golden/q15_reference.npz and q7_reference.npz hold
+ * outputs of the reference's own NEON kernels composed as its ESTIMATE
+ * plans (executed from their source text by tests/golden/neon_a64.py);
+ * tests/test_q15.py and tests/test_q7.py require this file to match them
+ * bit for bit.
+ *
+ * Data: interleaved (re, im) of int16 (Q0.15) or int8 (Q0.7), members
+ * idist/odist complex elements apart, unit element stride.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef struct {
+  int32_t re, im;
+} fc;
+
+/* lane format */
+typedef struct {
+  int bits;          /* 16 or 8 */
+  int32_t lo, hi;    /* saturation bounds */
+  int32_t one, mone; /* the constants 1 - 2^-(B-1) and -1 */
+  int32_t c8, c16, s16;
+} fmt;
+
+static fmt make_fmt(int bits);
+
+static int32_t sat(const fmt *f, int64_t v) { return v > f->hi ? f->hi : (v < f->lo ? f->lo : (int32_t)v); }
+static int32_t rshr(int32_t v, int s) { return (v + (1 << (s - 1))) >> s; }
+/* multiply by a real constant, one rounding */
+static int32_t rdm(const fmt *f, int32_t a, int32_t k) {
+  return sat(f, ((int64_t)a * k + ((int64_t)1 << (f->bits - 2))) >> (f->bits - 1));
+}
+/* two products accumulated in a 2B-bit lane (wrapping), one rounding narrow */
+static int32_t mac2(const fmt *f, int32_t a, int32_t ka, int32_t b, int32_t kb) {
+  const int w = 2 * f->bits;
+  int64_t acc = (int64_t)a * ka + (int64_t)b * kb;
+  const int64_t m = (int64_t)1 << w;
+  acc = ((acc % m) + m) % m;
+  if (acc >= m / 2) acc -= m;
+  return sat(f, (acc + ((int64_t)1 << (f->bits - 2))) >> (f->bits - 1));
+}
+
+static fc cadd(const fmt *f, fc a, fc b) { return (fc){sat(f, a.re + b.re), sat(f, a.im + b.im)}; }
+static fc csub(const fmt *f, fc a, fc b) { return (fc){sat(f, a.re - b.re), sat(f, a.im - b.im)}; }
+/* ~ i z and ~ -i z */
+static fc mul_pi(const fmt *f, fc z) { return (fc){rdm(f, z.im, f->mone), rdm(f, z.re, f->one)}; }
+static fc mul_mi(const fmt *f, fc z) { return (fc){rdm(f, z.im, f->one), rdm(f, z.re, f->mone)}; }
+
+/* ~ c (1 - i) z and ~ -c (1 + i) z, c = cos(pi/4): a real-constant product
+ * whose imaginary part is itself a rotated constant product, folded into one
+ * accumulate */
+static fc mul_w8(const fmt *f, fc z) {
+  return (fc){mac2(f, z.re, f->c8, rdm(f, z.im, f->c8), f->one),
+              mac2(f, z.im, f->c8, rdm(f, z.re, f->c8), f->mone)};
+}
+static fc mul_w8_3(const fmt *f, fc z) {
+  return (fc){mac2(f, z.re, -f->c8, rdm(f, z.im, -f->c8), f->mone),
+              mac2(f, z.im, -f->c8, rdm(f, z.re, -f->c8), f->one)};
+}
+/* (wr + i wi) z with one rounding per component */
+static fc mul_w(const fmt *f, fc z, int32_t wr, int32_t wi) {
+  return (fc){mac2(f, z.re, wr, z.im, -wi), mac2(f, z.im, wr, z.re, wi)};
+}
+
+/* ---- codelets: x[0..r) already pre-scaled; forward order ---- */
+static void dft2(const fmt *f, const fc *a, fc *y) {
+  y[0] = cadd(f, a[0], a[1]);
+  y[1] = csub(f, a[0], a[1]);
+}
+
+static void dft4(const fmt *f, const fc *a, fc *y) {
+  const fc s02 = cadd(f, a[0], a[2]), s13 = cadd(f, a[1], a[3]);
+  const fc d02 = csub(f, a[0], a[2]), j13 = mul_pi(f, csub(f, a[1], a[3]));
+  y[0] = cadd(f, s02, s13);
+  y[2] = csub(f, s02, s13);
+  y[1] = csub(f, d02, j13);
+  y[3] = cadd(f, d02, j13);
+}
+
+static void dft8(const fmt *f, const fc *a, fc *y) {
+  fc p[4], m[4];
+  for (int k = 0; k < 4; ++k) {
+    p[k] = cadd(f, a[k], a[k + 4]);
+    m[k] = csub(f, a[k], a[k + 4]);
+  }
+  const fc e0 = cadd(f, p[0], p[2]), e1 = cadd(f, p[1], p[3]);
+  y[0] = cadd(f, e0, e1);
+  y[4] = csub(f, e0, e1);
+  const fc d = csub(f, p[0], p[2]), jd = mul_pi(f, csub(f, p[1], p[3]));
+  y[2] = csub(f, d, jd);
+  y[6] = cadd(f, d, jd);
+  const fc z = cadd(f, m[1], m[3]), w = csub(f, m[1], m[3]);
+  const fc rd = {rdm(f, w.re, f->c8), rdm(f, w.im, f->c8)};
+  /* ~ i (M2 + c Z) and ~ i (M2 - c Z) */
+  const fc x = {mac2(f, m[2].im, f->mone, z.im, -f->c8), mac2(f, m[2].re, f->one, z.re, f->c8)};
+  const fc x2 = {mac2(f, m[2].im, f->mone, z.im, f->c8), mac2(f, m[2].re, f->one, z.re, -f->c8)};
+  const fc u = cadd(f, m[0], rd), v = csub(f, m[0], rd);
+  y[1] = csub(f, u, x);
+  y[7] = cadd(f, u, x);
+  y[3] = cadd(f, v, x2);
+  y[5] = csub(f, v, x2);
+}
+
+/* fixed-point split-radix 16 */
+static void dft16(const fmt *f, const fc *a, fc *y) {
+  fc p[8], m[8];
+  for (int k = 0; k < 8; ++k) {
+    p[k] = cadd(f, a[k], a[k + 8]);
+    m[k] = csub(f, a[k], a[k + 8]);
+  }
+  /* even outputs: length-8 split of p */
+  const fc s04 = cadd(f, p[0], p[4]), s26 = cadd(f, p[2], p[6]);
+  const fc s15 = cadd(f, p[1], p[5]), s37 = cadd(f, p[3], p[7]);
+  const fc e0 = cadd(f, s04, s26), e1 = cadd(f, s15, s37);
+  y[0] = cadd(f, e0, e1);
+  y[8] = csub(f, e0, e1);
+  const fc A = csub(f, s04, s26), jB = mul_pi(f, csub(f, s15, s37));
+  y[4] = csub(f, A, jB);
+  y[12] = cadd(f, A, jB);
+  const fc C = csub(f, p[0], p[4]), jD = mul_pi(f, csub(f, p[2], p[6]));
+  const fc kE = mul_w8(f, csub(f, p[1], p[5])), kF = mul_w8_3(f, csub(f, p[3], p[7]));
+  const fc g1 = csub(f, C, jD), g2 = cadd(f, C, jD);
+  const fc h = cadd(f, kE, kF), h2 = mul_mi(f, csub(f, kF, kE));
+  y[2] = cadd(f, g1, h);
+  y[10] = csub(f, g1, h);
+  y[6] = csub(f, g2, h2);
+  y[14] = cadd(f, g2, h2);
+  /* odd outputs */
+  const fc j4 = mul_pi(f, m[4]);
+  const fc q = csub(f, m[0], j4), q2 = cadd(f, m[0], j4);
+  const fc k2 = mul_w8(f, m[2]), k6 = mul_w8_3(f, m[6]);
+  const fc r = cadd(f, k2, k6), r2 = mul_mi(f, csub(f, k6, k2));
+  const fc j5 = mul_pi(f, m[5]), j7 = mul_pi(f, m[7]);
+  const fc u = csub(f, m[1], j5), u2 = cadd(f, m[1], j5);
+  const fc v = csub(f, m[3], j7), v2 = cadd(f, m[3], j7);
+  const fc l1 = mul_w(f, u, f->c16, -f->s16), l3 = mul_w(f, v, f->s16, -f->c16);
+  const fc l3b = mul_w(f, u2, f->s16, -f->c16), l9 = mul_w(f, v2, -f->c16, f->s16);
+  const fc qr = cadd(f, q, r), qmr = csub(f, q, r);
+  const fc ls = cadd(f, l1, l3), ld = mul_mi(f, csub(f, l3, l1));
+  y[1] = cadd(f, qr, ls);
+  y[9] = csub(f, qr, ls);
+  y[5] = csub(f, qmr, ld);
+  y[13] = cadd(f, qmr, ld);
+  const fc qa = csub(f, q2, r2), qb = cadd(f, q2, r2);
+  const fc ls2 = cadd(f, l3b, l9), ld2 = mul_mi(f, csub(f, l9, l3b));
+  y[3] = cadd(f, qa, ls2);
+  y[11] = csub(f, qa, ls2);
+  y[7] = csub(f, qb, ld2);
+  y[15] = cadd(f, qb, ld2);
+}
+
+static int ilog2(int r) {
+  int s = 0;
+  while ((1 << s) < r) ++s;
+  return s;
+}
+
+/* one codelet of length r on pre-scaled inputs; the backward codelet
+ * returns the forward one's outputs in reversed index order */
+static void codelet(const fmt *f, int r, int dir, const fc *a, fc *out) {
+  fc y[16];
+  switch (r) {
+    case 1: y[0] = a[0]; break;
+    case 2: dft2(f, a, y); break;
+    case 4: dft4(f, a, y); break;
+    case 8: dft8(f, a, y); break;
+    default: dft16(f, a, y); break;
+  }
+  for (int k = 0; k < r; ++k) out[k] = y[dir < 0 ? k : (r - k) % r];
+}
+
+static int32_t cvt(const fmt *f, double x) {
+  const float v = (float)x * (float)(1 << (f->bits - 1));
+  return sat(f, (int64_t)trunc((double)v));
+}
+
+static fmt make_fmt(int bits) {
+  fmt f;
+  f.bits = bits;
+  f.hi = (1 << (bits - 1)) - 1;
+  f.lo = -(1 << (bits - 1));
+  f.one = f.hi;
+  f.mone = f.lo;
+  f.c8 = cvt(&f, cos(M_PI / 4));
+  f.c16 = cvt(&f, cos(M_PI / 8));
+  f.s16 = cvt(&f, sin(M_PI / 8));
+  return f;
+}
+
+/* premultiplied twiddle table of a radix-16 level over n1 rows, angle
+ * dir 2 pi i j / (16 n1): for j = 1..n1-1, i = 1..15: (c, s, cvt(-s), c) */
+static void twiddles16(const fmt *f, int64_t n1, int dir, int32_t *w) {
+  const double base = (double)dir * 2.0 * M_PI / (double)(16 * n1);
+  int64_t x = 0;
+  for (int64_t j = 1; j < n1; ++j)
+    for (int64_t i = 1; i < 16; ++i) {
+      const double ang = base * (double)i * (double)j;
+      const double a = cos(ang), b = sin(ang);
+      w[x++] = cvt(f, a);
+      w[x++] = cvt(f, b);
+      w[x++] = cvt(f, -b);
+      w[x++] = cvt(f, a);
+    }
+}
+
+/* a 16-point codelet on pre-scaled inputs, the inputs i >= 1 multiplied by
+ * row `row` of a premultiplied table (row 0: untwiddled) */
+static void twiddled16(const fmt *f, int dir, const fc *v, int64_t row, const int32_t *w, fc *out) {
+  fc a[16];
+  for (int i = 0; i < 16; ++i) {
+    const fc s = {rshr(v[i].re, 4), rshr(v[i].im, 4)};
+    if (row == 0 || i == 0) {
+      a[i] = s;
+    } else {
+      const int32_t *t = w + 4 * (15 * (row - 1) + (i - 1));
+      a[i] = (fc){mac2(f, s.re, t[0], s.im, t[2]), mac2(f, s.re, t[1], s.im, t[3])};
+    }
+  }
+  codelet(f, 16, dir, a, out);
+}
+
+typedef struct {
+  const fmt *f;
+  int bits;
+  const void *in;
+  void *out;
+} io;
+
+static fc ld(int bits, const void *p, int64_t k) {
+  if (bits == 16) {
+    const int16_t *q = (const int16_t *)p;
+    return (fc){q[2 * k], q[2 * k + 1]};
+  }
+  const int8_t *q = (const int8_t *)p;
+  return (fc){q[2 * k], q[2 * k + 1]};
+}
+static void st(int bits, void *p, int64_t k, fc v) {
+  if (bits == 16) {
+    int16_t *q = (int16_t *)p;
+    q[2 * k] = (int16_t)v.re;
+    q[2 * k + 1] = (int16_t)v.im;
+  } else {
+    int8_t *q = (int8_t *)p;
+    q[2 * k] = (int8_t)v.re;
+    q[2 * k + 1] = (int8_t)v.im;
+  }
+}
+
+/* fixed-point C2C of power-of-two n in [1, 4096]; returns 0, or -1 if n is
+ * not supported */
+static int fixed_c2c(int bits, const void *in, void *out, int64_t n, int64_t howmany, int64_t idist,
+                     int64_t odist, int dir) {
+  if (n < 1 || n > 4096 || (n & (n - 1))) return -1;
+  const fmt F = make_fmt(bits), *f = &F;
+  const size_t esz = (size_t)(bits / 4); /* bytes per complex element */
+  if (n <= 16) {
+    const int s = ilog2((int)n);
+    for (int64_t b = 0; b < howmany; ++b) {
+      fc a[16], y[16];
+      const void *x = (const char *)in + esz * (size_t)(b * idist);
+      for (int k = 0; k < n; ++k) {
+        const fc v = ld(bits, x, k);
+        a[k] = s ? (fc){rshr(v.re, s), rshr(v.im, s)} : v;
+      }
+      codelet(f, (int)n, dir, a, y);
+      for (int k = 0; k < n; ++k) st(bits, (char *)out + esz * (size_t)(b * odist), k, y[k]);
+    }
+    return 0;
+  }
+  const int64_t m = n / 16;                        /* rows of the outer radix-16 level */
+  const int64_t m2 = n > 256 ? n / 256 : 0;        /* rows of the inner radix-16 level */
+  const int64_t first = n > 256 ? m2 : m;          /* length of the first-stage codelets */
+  const int64_t cols = n / first;                  /* number of first-stage columns */
+  const int sf = ilog2((int)first);
+  int32_t *w = (int32_t *)malloc(sizeof(int32_t) * 4 * 15 * (size_t)(m > 1 ? m - 1 : 1));
+  int32_t *w2 = (int32_t *)malloc(sizeof(int32_t) * 4 * 15 * (size_t)(m2 > 1 ? m2 - 1 : 1));
+  fc *b1 = (fc *)malloc(sizeof(fc) * (size_t)n);
+  fc *b0 = (fc *)malloc(sizeof(fc) * (size_t)n);
+  twiddles16(f, m, dir, w);
+  if (m2) twiddles16(f, m2, dir, w2);
+  for (int64_t b = 0; b < howmany; ++b) {
+    const void *x = (const char *)in + esz * (size_t)(b * idist);
+    void *yb = (char *)out + esz * (size_t)(b * odist);
+    /* first stage: length-`first` codelets down the columns x[c + cols q] */
+    for (int64_t c = 0; c < cols; ++c) {
+      fc a[16], y[16];
+      for (int q = 0; q < first; ++q) {
+        const fc v = ld(bits, x, c + cols * q);
+        a[q] = (fc){rshr(v.re, sf), rshr(v.im, sf)};
+      }
+      codelet(f, (int)first, dir, a, y);
+      for (int k = 0; k < first; ++k) b1[c + cols * k] = y[k];
+    }
+    const fc *rows = b1;
+    if (m2) { /* inner radix-16 level: column t, row i0 */
+      for (int64_t i0 = 0; i0 < m2; ++i0)
+        for (int t = 0; t < 16; ++t) {
+          fc v[16], y[16];
+          for (int i = 0; i < 16; ++i) v[i] = b1[256 * i0 + t + 16 * i];
+          twiddled16(f, dir, v, i0, w2, y);
+          for (int k = 0; k < 16; ++k) b0[16 * i0 + t + 16 * m2 * k] = y[k];
+        }
+      rows = b0;
+    }
+    for (int64_t j = 0; j < m; ++j) { /* outer radix-16 level: twiddled rows */
+      fc y[16];
+      twiddled16(f, dir, rows + 16 * j, j, w, y);
+      for (int k = 0; k < 16; ++k) st(bits, yb, j + m * k, y[k]);
+    }
+  }
+  free(w);
+  free(w2);
+  free(b1);
+  free(b0);
+  return 0;
+}
+
+int oracle_q15_c2c(const int16_t *in, int16_t *out, int64_t n, int64_t howmany, int64_t idist, int64_t odist,
+                   int dir) {
+  return fixed_c2c(16, in, out, n, howmany, idist, odist, dir);
+}
+
+int oracle_q7_c2c(const int8_t *in, int8_t *out, int64_t n, int64_t howmany, int64_t idist, int64_t odist,
+                  int dir) {
+  return fixed_c2c(8, in, out, n, howmany, idist, odist, dir);
+}
+
+/* the outer radix-16 level's Q0.15 twiddle table for length n (n / 16 rows),
+ * as int16: (c, s, cvt(-s), c) per (row, input) */
+void oracle_q15_twiddles(int64_t n, int dir, int16_t *w) {
+  const fmt F = make_fmt(16);
+  const int64_t m = n / 16;
+  int32_t *t = (int32_t *)malloc(sizeof(int32_t) * 4 * 15 * (size_t)(m > 1 ? m - 1 : 1));
+  twiddles16(&F, m, dir, t);
+  for (int64_t i = 0; i < 4 * 15 * (m - 1); ++i) w[i] = (int16_t)t[i];
+  free(t);
+}

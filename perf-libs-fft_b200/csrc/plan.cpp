@@ -187,10 +187,12 @@ struct C2CPow2Node : Node {
   // test hook (PLFFT_B200_TEST_STALL_CTA): the CTA whose first load is
   // withheld in the next run only
   mutable std::atomic<int> stall_once{-1};
+  uint64_t stall_wait_ns = 0;  // the shortened wait limit of that run
   void status_words(std::vector<int*>& out) const override { out.push_back(status.p); }
   cudaError_t run(const void* in, void* out, void*, cudaStream_t st) const override {
     Pow2Launch L = base;
     L.stall_cta = stall_once.exchange(-1);
+    if (L.stall_cta >= 0) L.wait_ns = stall_wait_ns;
     L.in = static_cast<const float2*>(in);
     L.out = static_cast<float2*>(out);
     const bool dist_in_ok = L.howmany == 1 || (L.idist % 2) == 0;
@@ -262,7 +264,7 @@ static std::unique_ptr<Node> make_pow2(int64_t n, const Layout& lay, int dir, fl
   // PLFFT_DEVICE_TIMEOUT; nothing is in flight when that CTA leaves.
   if (const char* v = std::getenv("PLFFT_B200_TEST_STALL_CTA")) {
     node->stall_once = std::atoi(v);
-    node->base.wait_ns = uint64_t(std::max(1, env_int("PLFFT_B200_TEST_WAIT_US", 2000))) * 1000u;
+    node->stall_wait_ns = uint64_t(std::max(1, env_int("PLFFT_B200_TEST_WAIT_US", 2000))) * 1000u;
   }
   // CTA ring, one transform per CTA for n = 1024 (g = 32 / T), 3 slots:
   // measured best at batch 4096 (4.09 TB/s; deeper rings, twiddles in

@@ -1,15 +1,24 @@
-"""Interpreter for the AArch64/NEON instruction subset of PLFFT's Q0.15 kernels.
+"""Interpreter for the AArch64 / NEON instruction subset of PLFFT's kernels.
 
-Test infrastructure only: make_q15_golden.py uses it, in the container that
-holds the reference sources, to execute the reference's own generated q15
-kernels (src/providers/aot/asm/neon/plfft_*q15*.S, read as text) on seeded
-inputs.  The outputs become the committed fixture tests/golden/q15_reference.npz
-that pins the bit-exact Q0.15 path.  Nothing at test time reads the reference.
+Test infrastructure only: the fixture generators in this folder use it, in
+a container that holds the reference sources, to execute the reference's
+own generated NEON kernels (src/providers/aot/asm/neon/*.S, read as text)
+on seeded inputs.  Their outputs become committed fixtures; nothing at test
+time reads the reference.
 
-Semantics implemented (Arm A64 definitions): integer loads/stores of
-S/D/Q/X registers, address arithmetic, compare-and-branch, and the vector
-ops sqadd, sqsub, srshr, sqrdmulh, smull(2), smlal(2), smlsl(2) (vector and
-by-element), sqrshrn(2), rev32, zip1, trn1, trn2.
+Semantics implemented (Arm A64 definitions):
+  scalar  ldr/str (B/H/S/D/Q and X registers), ldp/stp, add/sub (immediate,
+          register, shifted register), lsl, asr, mul, movz, mov, cmp,
+          b / b.lt / b.ge, ret, adrp + page offsets of read-only data
+  loads   ld1r (replicate one element to every lane), dup (by element)
+  FP32    fadd, fsub, fmul (vector and by element), fmla / fmls (vector and
+          by element; a fused multiply-add rounded once: the product is
+          exact in double, the sum is formed with an exact two-sum and
+          rounded to single precision once, ties broken by the two-sum's
+          error term)
+  integer sqadd, sqsub, srshr, sqrdmulh, smull(2), smlal(2), smlsl(2)
+          (vector and by element), sqrshrn(2) on 8- and 16-bit lanes
+  permute rev16, rev32, rev64, zip1, trn1, trn2
 """
 import re
 
@@ -17,18 +26,19 @@ import numpy as np
 
 MASK64 = (1 << 64) - 1
 
+# lane arrangement -> (lanes, bytes per lane)
+_ARR = {"8b": (8, 1), "16b": (16, 1), "4h": (4, 2), "8h": (8, 2), "2s": (2, 4), "4s": (4, 4),
+        "1d": (1, 8), "2d": (2, 8)}
+_INT = {1: np.int8, 2: np.int16, 4: np.int32, 8: np.int64}
+
 
 def _s64(v):
     v &= MASK64
     return v - (1 << 64) if v >> 63 else v
 
 
-def _sat16(a):
-    return np.clip(a, -32768, 32767)
-
-
 class Kernels:
-    """Parsed functions (name -> instruction list) and read-only data."""
+    """Parsed functions (name -> instruction list), labels and read-only data."""
 
     def __init__(self, paths):
         self.funcs, self.labels, self.rodata = {}, {}, {}
@@ -68,9 +78,9 @@ class Kernels:
 def _split_operands(s):
     out, depth, cur = [], 0, ""
     for ch in s:
-        if ch == "[":
+        if ch in "[{":
             depth += 1
-        elif ch == "]":
+        elif ch in "]}":
             depth -= 1
         if ch == "," and depth == 0:
             out.append(cur)
@@ -80,6 +90,28 @@ def _split_operands(s):
     if cur.strip():
         out.append(cur)
     return out
+
+
+def _fma32(a, b, d, negate=False):
+    """float32 d + a*b (or d - a*b) rounded once, elementwise."""
+    p = a.astype(np.float64) * b.astype(np.float64)  # exact
+    if negate:
+        p = -p
+    dd = d.astype(np.float64)
+    s = p + dd
+    bb = s - p
+    e = (p - (s - bb)) + (dd - bb)  # s + e == p + d exactly (two-sum)
+    r = s.astype(np.float32)
+    r64 = r.astype(np.float64)
+    # |e| is at most half an ulp of s in double, so s + e rounds like s unless
+    # s sits exactly halfway between r and its neighbour nb on s's side;
+    # then the sign of e decides
+    nb = np.where(s > r64, np.nextafter(r, np.float32(np.inf)), np.nextafter(r, np.float32(-np.inf)))
+    at_mid = (s == (r64 + nb.astype(np.float64)) * 0.5) & (e != 0)
+    if np.any(at_mid):
+        toward_nb = np.sign(e) == np.sign(nb.astype(np.float64) - r64)
+        r = np.where(at_mid & toward_nb, nb, r)
+    return r.astype(np.float32)
 
 
 class Machine:
@@ -115,7 +147,6 @@ class Machine:
         self.x = [0] * 31
         self.sp = self.stack_top
         self.v = [np.zeros(16, np.uint8) for _ in range(32)]
-        self.nzcv = 0
         for i, a in enumerate(args):
             self.x[i] = int(a) & MASK64
         code = self.k.funcs[name]
@@ -143,7 +174,8 @@ class Machine:
         elif s != "xzr":
             self.x[int(s[1:])] = val & MASK64
 
-    def imm(self, s):
+    @staticmethod
+    def imm(s):
         return int(s.lstrip("#"), 0)
 
     def addr(self, s):
@@ -161,31 +193,40 @@ class Machine:
         return base + off
 
     def vreg(self, s):
-        return self.v[int(re.match(r"[vqsdh](\d+)", s).group(1))]
+        return self.v[int(re.match(r"\{?[vqsdhb](\d+)", s).group(1))]
 
     @staticmethod
     def arr(s):
-        return s.split(".")[1] if "." in s else None
+        return s.split(".")[1].rstrip("}") if "." in s else None
 
-    def lanes16(self, s):
-        """int64 array of the 16-bit lanes named by an arrangement (4h -> 4, 8h -> 8)."""
+    def lanes(self, s, kind="i"):
+        """The lanes of a register operand as int64 ('i') or float32 ('f')."""
+        n, w = _ARR[self.arr(s)]
         r = self.vreg(s)
-        n = 8 if self.arr(s) == "8h" else 4
-        return r.view(np.int16)[:n].astype(np.int64)
+        if kind == "f":
+            return r.view(np.float32)[:n].copy()
+        return r.view(_INT[w])[:n].astype(np.int64)
 
-    def put16(self, s, vals, clear_hi=True):
+    def put(self, s, vals, kind="i"):
+        n, w = _ARR[self.arr(s)]
         r = self.vreg(s)
-        n = 8 if self.arr(s) == "8h" else 4
-        r.view(np.int16)[:n] = vals.astype(np.int16)
-        if n == 4 and clear_hi:
+        if kind == "f":
+            r.view(np.float32)[:n] = vals
+        else:
+            r.view(_INT[w])[:n] = np.asarray(vals).astype(_INT[w])
+        if n * w == 8:
             r[8:] = 0
 
-    def elem16(self, s):
-        m = re.match(r"v(\d+)\.h\[(\d+)\]", s)
-        return int(self.v[int(m.group(1))].view(np.int16)[int(m.group(2))])
+    def elem(self, s, kind="i"):
+        m = re.match(r"v(\d+)\.([bhsd])\[(\d+)\]", s)
+        r = self.v[int(m.group(1))]
+        i = int(m.group(3))
+        if kind == "f":
+            return r.view(np.float32)[i]
+        return int(r.view(_INT[{"b": 1, "h": 2, "s": 4, "d": 8}[m.group(2)]])[i])
 
     # ---------------------------------------------------------------
-    _VBYTES = {"s": 4, "d": 8, "q": 16}
+    _VBYTES = {"b": 1, "h": 2, "s": 4, "d": 8, "q": 16}
 
     def step(self, fname, op, o):
         if op in ("ldr", "str"):
@@ -211,6 +252,14 @@ class Machine:
                     self.setreg(r, int(self.mem[a + 8 * i:a + 8 * i + 8].view(np.uint64)[0]))
                 else:
                     self.mem[a + 8 * i:a + 8 * i + 8] = np.array([self.reg(r)], np.uint64).view(np.uint8)
+            return None
+        if op == "ld1r":
+            n, w = _ARR[self.arr(o[0])]
+            a = self.addr(o[1])
+            v = self.vreg(o[0])
+            v[:] = np.tile(self.mem[a:a + w], 16 // w)
+            if n * w == 8:
+                v[8:] = 0
             return None
         if op == "adrp":
             self.setreg(o[0], self.ro_addr[re.search(r"\((.*)\)", o[1]).group(1)])
@@ -254,67 +303,90 @@ class Machine:
 
     def vstep(self, op, o):
         d = o[0]
-        if op in ("sqadd", "sqsub"):
-            a, b = self.lanes16(o[1]), self.lanes16(o[2])
-            self.put16(d, _sat16(a + b if op == "sqadd" else a - b))
+        if op in ("fadd", "fsub", "fmul", "fmla", "fmls"):
+            a = self.lanes(o[1], "f")
+            b = np.float32(self.elem(o[2], "f")) if "[" in o[2] else self.lanes(o[2], "f")
+            b = np.broadcast_to(np.asarray(b, np.float32), a.shape)
+            if op == "fadd":
+                r = a + b
+            elif op == "fsub":
+                r = a - b
+            elif op == "fmul":
+                r = a * b
+            else:
+                r = _fma32(a, b, self.lanes(d, "f"), negate=op == "fmls")
+            self.put(d, r.astype(np.float32), "f")
+        elif op in ("sqadd", "sqsub"):
+            _, w = _ARR[self.arr(d)]
+            lo, hi = -(1 << (8 * w - 1)), (1 << (8 * w - 1)) - 1
+            a, b = self.lanes(o[1]), self.lanes(o[2])
+            self.put(d, np.clip(a + b if op == "sqadd" else a - b, lo, hi))
         elif op == "srshr":
             s = self.imm(o[2])
-            self.put16(d, (self.lanes16(o[1]) + (1 << (s - 1))) >> s)
+            self.put(d, (self.lanes(o[1]) + (1 << (s - 1))) >> s)
         elif op == "sqrdmulh":
-            a = self.lanes16(o[1])
-            b = self.elem16(o[2]) if "[" in o[2] else self.lanes16(o[2])
-            self.put16(d, _sat16((2 * a * b + (1 << 15)) >> 16))
+            _, w = _ARR[self.arr(d)]
+            bits = 8 * w
+            a = self.lanes(o[1])
+            b = self.elem(o[2]) if "[" in o[2] else self.lanes(o[2])
+            r = (2 * a * b + (1 << (bits - 1))) >> bits
+            self.put(d, np.clip(r, -(1 << (bits - 1)), (1 << (bits - 1)) - 1))
         elif op in ("smull", "smull2", "smlal", "smlal2", "smlsl", "smlsl2"):
             hi = op.endswith("2")
-            a = self.vreg(o[1]).view(np.int16)[4:8 if hi else 4].astype(np.int64) if hi else \
-                self.vreg(o[1]).view(np.int16)[:4].astype(np.int64)
+            nd, wd = _ARR[self.arr(d)]
+            src = self.vreg(o[1]).view(_INT[wd // 2])
+            a = (src[nd:2 * nd] if hi else src[:nd]).astype(np.int64)
             if "[" in o[2]:
-                b = self.elem16(o[2])
+                b = self.elem(o[2])
             else:
-                bv = self.vreg(o[2]).view(np.int16)
-                b = (bv[4:8] if hi else bv[:4]).astype(np.int64)
+                bv = self.vreg(o[2]).view(_INT[wd // 2])
+                b = (bv[nd:2 * nd] if hi else bv[:nd]).astype(np.int64)
             prod = a * b
-            acc = self.vreg(d).view(np.int32).astype(np.int64)
+            acc = self.vreg(d).view(_INT[wd])[:nd].astype(np.int64)
             if op.startswith("smull"):
                 res = prod
             elif op.startswith("smlal"):
                 res = acc + prod
             else:
                 res = acc - prod
-            res = ((res + (1 << 31)) % (1 << 32)) - (1 << 31)  # 32-bit wrap
-            self.vreg(d).view(np.int32)[:] = res.astype(np.int32)
+            m = 1 << (8 * wd)
+            res = ((res + m // 2) % m) - m // 2  # wraps at the lane width
+            self.vreg(d).view(_INT[wd])[:nd] = res.astype(_INT[wd])
         elif op in ("sqrshrn", "sqrshrn2"):
             s = self.imm(o[2])
-            a = self.vreg(o[1]).view(np.int32).astype(np.int64)
-            r = _sat16((a + (1 << (s - 1))) >> s).astype(np.int16)
-            v = self.vreg(d)
+            ns_, ws = _ARR[self.arr(o[1])]
+            a = self.vreg(o[1]).view(_INT[ws])[:ns_].astype(np.int64)
+            bits = 4 * ws
+            r = np.clip((a + (1 << (s - 1))) >> s, -(1 << (bits - 1)), (1 << (bits - 1)) - 1)
+            v = self.vreg(d).view(_INT[ws // 2])
             if op == "sqrshrn":
-                v.view(np.int16)[:4] = r
-                v[8:] = 0
+                v[:ns_] = r
+                self.vreg(d)[8:] = 0
             else:
-                v.view(np.int16)[4:8] = r
-        elif op == "rev32":
-            a = self.lanes16(o[1])
-            sw = a.reshape(-1, 2)[:, ::-1].ravel()
-            self.put16(d, sw)
+                v[ns_:2 * ns_] = r
+        elif op in ("rev16", "rev32", "rev64"):
+            n, w = _ARR[self.arr(d)]
+            group = {"rev16": 2, "rev32": 4, "rev64": 8}[op] // w
+            a = self.vreg(o[1]).view(_INT[w])[:n].copy()
+            self.put(d, a.reshape(-1, group)[:, ::-1].ravel().astype(np.int64))
         elif op == "zip1":
-            t = self.arr(d)
-            n, m = self.vreg(o[1]).copy(), self.vreg(o[2]).copy()
-            v = self.vreg(d)
-            if t == "2s":
-                v[:] = 0
-                v[0:4], v[4:8] = n[0:4], m[0:4]
-            elif t == "2d":
-                v[0:8], v[8:16] = n[0:8], m[0:8]
-            else:
-                raise NotImplementedError(f"zip1 .{t}")
+            n, w = _ARR[self.arr(d)]
+            a = self.vreg(o[1]).view(_INT[w])[:n].copy()
+            b = self.vreg(o[2]).view(_INT[w])[:n].copy()
+            r = np.empty(n, _INT[w])
+            r[0::2], r[1::2] = a[: n // 2], b[: n // 2]
+            self.put(d, r.astype(np.int64))
         elif op in ("trn1", "trn2"):
-            n = self.vreg(o[1]).view(np.int16).copy()
-            m = self.vreg(o[2]).view(np.int16).copy()
+            n, w = _ARR[self.arr(d)]
+            a = self.vreg(o[1]).view(_INT[w])[:n].copy()
+            b = self.vreg(o[2]).view(_INT[w])[:n].copy()
             off = 0 if op == "trn1" else 1
-            r = np.empty(8, np.int16)
-            r[0::2], r[1::2] = n[off::2], m[off::2]
-            self.vreg(d).view(np.int16)[:] = r
+            r = np.empty(n, _INT[w])
+            r[0::2], r[1::2] = a[off::2], b[off::2]
+            self.put(d, r.astype(np.int64))
+        elif op == "dup":
+            n, w = _ARR[self.arr(d)]
+            self.put(d, np.full(n, self.elem(o[1]), np.int64))
         else:
             raise NotImplementedError(op)
         return None

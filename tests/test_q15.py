@@ -2,8 +2,9 @@
 
 tests/golden/q15_reference.npz holds outputs of the reference's own NEON
 Q0.15 kernels (src/providers/aot/asm/neon/plfft_*q15*.S), executed from
-their source text by tests/golden/neon_q15.py and composed as the
-reference's ESTIMATE plan by tests/golden/make_q15_golden.py.  The C
+their source text by tests/golden/neon_a64.py and composed as the
+reference's ESTIMATE plan by tests/golden/ref_c2c_plan.py
+(tests/golden/make_ref_golden.py).  The C
 restatement oracle/q15.c must reproduce them bit for bit.  It must also
 meet the reference's own fixed-point accuracy bound: 6 * log2(n) LSB
 against the exact DFT scaled by 1/n (test/test_utils.hpp:131-152).
@@ -16,7 +17,7 @@ import pytest
 import oracle
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "q15_reference.npz")
-SIZES = [2, 4, 8, 16, 32, 64, 128, 256]
+SIZES = [2, 4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096]
 
 
 @pytest.fixture(scope="module")
@@ -82,32 +83,34 @@ def test_q15_twiddle_table_conversion():
 # codelets (sums, sqrdmulh constants, 32-bit MACs) and no twiddled row input
 # can leave int16; only the outputs y_k can saturate.
 # ---------------------------------------------------------------------------
-def _saturating_ops():
+def _saturating_ops(bits=16):
     class I:
         def __init__(s, lo, hi): s.lo, s.hi = lo, hi
         def __add__(s, o): return I(s.lo + o.lo, s.hi + o.hi)
         def __sub__(s, o): return I(s.lo - o.hi, s.hi - o.lo)
         def __repr__(s): return f"[{s.lo},{s.hi}]"
-    def sat(x): return I(max(-32768, min(32767, x.lo)), max(-32768, min(32767, x.hi)))
+    LO, HI = -(1 << (bits - 1)), (1 << (bits - 1)) - 1
+    def sat(x): return I(max(LO, min(HI, x.lo)), max(LO, min(HI, x.hi)))
     need = {}
     def chk(tag, x):
-        if x.lo < -32768 or x.hi > 32767: need[tag] = need.get(tag, 0) + 1
+        if x.lo < LO or x.hi > HI: need[tag] = need.get(tag, 0) + 1
         else: need.setdefault(tag, 0)
         return sat(x)
     def add(tag, a, b): return (chk(tag + '.re', a[0] + b[0]), chk(tag + '.im', a[1] + b[1]))
     def sub(tag, a, b): return (chk(tag + '.re', a[0] - b[0]), chk(tag + '.im', a[1] - b[1]))
     def mulk(x, k):  # exact product interval
         c = [x.lo * k, x.hi * k]; return I(min(c), max(c))
-    def rdm(x, k): p = mulk(x, 2 * k); return I((p.lo + 32768) >> 16, (p.hi + 32768) >> 16)
+    def rdm(x, k): p = mulk(x, k); return I((p.lo + (1 << (bits - 2))) >> (bits - 1), (p.hi + (1 << (bits - 2))) >> (bits - 1))
     def rdmt(tag, x, k): return chk(tag, rdm(x, k))
     def mac(tag, a, ka, b, kb):
         s = mulk(a, ka) + mulk(b, kb)
-        return chk(tag, I((s.lo + 16384) >> 15, (s.hi + 16384) >> 15))
-    def mul_pi(t, z): return (rdmt(t + '.pr', z[1], -32768), rdmt(t + '.pi', z[0], 32767))
-    def mul_mi(t, z): return (rdmt(t + '.mr', z[1], 32767), rdmt(t + '.mi', z[0], -32768))
-    C8, C16, S16 = 23170, 30273, 12539
-    def w8(t, z): return (mac(t + '.w8r', z[0], C8, rdm(z[1], C8), 32767), mac(t + '.w8i', z[1], C8, rdm(z[0], C8), -32768))
-    def w83(t, z): return (mac(t + '.w83r', z[0], -C8, rdm(z[1], -C8), -32768), mac(t + '.w83i', z[1], -C8, rdm(z[0], -C8), 32767))
+        assert -(1 << (2 * bits - 1)) <= s.lo and s.hi < (1 << (2 * bits - 1)), tag  # no lane wrap
+        return chk(tag, I((s.lo + (1 << (bits - 2))) >> (bits - 1), (s.hi + (1 << (bits - 2))) >> (bits - 1)))
+    def mul_pi(t, z): return (rdmt(t + '.pr', z[1], LO), rdmt(t + '.pi', z[0], HI))
+    def mul_mi(t, z): return (rdmt(t + '.mr', z[1], HI), rdmt(t + '.mi', z[0], LO))
+    C8, C16, S16 = (23170, 30273, 12539) if bits == 16 else (90, 118, 48)
+    def w8(t, z): return (mac(t + '.w8r', z[0], C8, rdm(z[1], C8), HI), mac(t + '.w8i', z[1], C8, rdm(z[0], C8), LO))
+    def w83(t, z): return (mac(t + '.w83r', z[0], -C8, rdm(z[1], -C8), LO), mac(t + '.w83i', z[1], -C8, rdm(z[0], -C8), HI))
     def mw(t, z, wr, wi): return (mac(t + '.r', z[0], wr, z[1], -wi), mac(t + '.i', z[1], wr, z[0], wi))
     def dft16(a):
         p = [add(f'p{k}', a[k], a[k + 8]) for k in range(8)]; m = [sub(f'm{k}', a[k], a[k + 8]) for k in range(8)]
@@ -133,23 +136,23 @@ def _saturating_ops():
         e0 = add('8e0', p[0], p[2]); e1 = add('8e1', p[1], p[3]); add('8y0', e0, e1); sub('8y4', e0, e1)
         d = sub('8d', p[0], p[2]); jd = mul_pi('8jd', sub('8ds', p[1], p[3])); sub('8y2', d, jd); add('8y6', d, jd)
         z = add('8z', m[1], m[3]); w = sub('8w', m[1], m[3]); rd = (rdmt('8rdr', w[0], C8), rdmt('8rdi', w[1], C8))
-        x = (mac('8xr', m[2][1], -32768, z[1], -C8), mac('8xi', m[2][0], 32767, z[0], C8))
-        x2 = (mac('8x2r', m[2][1], -32768, z[1], C8), mac('8x2i', m[2][0], 32767, z[0], -C8))
+        x = (mac('8xr', m[2][1], LO, z[1], -C8), mac('8xi', m[2][0], HI, z[0], C8))
+        x2 = (mac('8x2r', m[2][1], LO, z[1], C8), mac('8x2i', m[2][0], HI, z[0], -C8))
         u = add('8u', m[0], rd); v = sub('8v', m[0], rd)
         sub('8y1', u, x); add('8y7', u, x); add('8y3', v, x2); sub('8y5', v, x2)
     def dft4(a):
         s02 = add('4s02', a[0], a[2]); s13 = add('4s13', a[1], a[3]); d02 = sub('4d02', a[0], a[2]); j13 = mul_pi('4j13', sub('4d13', a[1], a[3]))
         add('4y0', s02, s13); sub('4y2', s02, s13); sub('4y1', d02, j13); add('4y3', d02, j13)
     def dft2(a): add('2y0', a[0], a[1]); sub('2y1', a[0], a[1])
-    def pre(s):  # rounding shift of any int16
-        return I((-32768 + (1 << (s - 1))) >> s, (32767 + (1 << (s - 1))) >> s)
+    def pre(s):  # rounding shift of any lane value
+        return I((LO + (1 << (s - 1))) >> s, (HI + (1 << (s - 1))) >> s)
     for r, f in ((2, dft2), (4, dft4), (8, dft8), (16, dft16)):
         s = r.bit_length() - 1
         a = [(pre(s), pre(s))] * r
         f(a)
     # twiddled row inputs: mac of pre-shifted values with arbitrary int16 twiddles
     t = pre(4)
-    mac('tw.re', t, 32767, t, -32768); mac('tw.re2', t, -32768, t, -32768)
+    mac('tw.re', t, HI, t, LO); mac('tw.re2', t, LO, t, LO)
     return need
 
 
@@ -158,4 +161,13 @@ def test_q15_codelet_intermediates_never_saturate():
     can = sorted(k for k, v in need.items() if v)
     assert len(need) > 200
     # every op that can saturate is a codelet output (named y*, 2y*, 4y*, 8y*)
+    assert can and all(k.lstrip("248").startswith("y") for k in can), can
+
+
+def test_q7_codelet_intermediates_never_saturate():
+    """The same interval analysis for Q0.7 lanes (8-bit values, 16-bit MAC
+    lanes that must not wrap): only codelet outputs can saturate."""
+    need = _saturating_ops(8)
+    can = sorted(k for k, v in need.items() if v)
+    assert len(need) > 200
     assert can and all(k.lstrip("248").startswith("y") for k in can), can
