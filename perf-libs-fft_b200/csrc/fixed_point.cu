@@ -1,0 +1,439 @@
+// Fixed-point C2C, Q0.15 (B = 16) and Q0.7 (B = 8), power-of-two n <= 4096,
+// bit-exact to the reference's NEON fixed-point path.
+//
+// Arithmetic (reference src/providers/jit/print_algo.cpp:1228-1230,
+// src/providers/jit/emit.hpp:150-175 and :370-425, constant lowering
+// print_algo.cpp:2150-2290): codelet inputs are pre-scaled by a rounding
+// shift right by log2(radix); additions saturate to B bits; a real-constant
+// multiply is (a k + 2^(B-2)) >> (B-1) (sqrdmulh for Q0.15, smull + sqrshrn
+// #7 for Q0.7); a twiddle product is two B x B products accumulated in a
+// 2B-bit lane and narrowed by one rounding, saturating shift by B - 1.  The
+// codelets are radix 2, 4, 8 and the fixed-point split-radix 16
+// (src/providers/jit/split_radix_z16.cpp, src/providers/jit/wfta_nfact.cpp:
+// 89-97); a backward codelet of length r yields the forward codelet's
+// output r-k at index k.  Decomposition = the reference's ESTIMATE plan
+// (planner/planner.cpp:51-175 with base kernels {2, 4, 8, 16}):
+//   n <= 16     one codelet;
+//   n = 16 m    cooley_tukey_ab(16) (planner/strategies/cooley_tukey.hpp:
+//               82-143, 622-680): length-m codelets down the 16 columns
+//               x[c + 16 q], then per row j a 16-point codelet whose inputs
+//               i >= 1 are multiplied by the twiddle of W_n^{dir i j},
+//               output y[j + m k];
+//   n = 256 m'  the length-16 m' sub-transforms of that plan are
+//               cooley_tukey_ac(16) (cooley_tukey.hpp:331-385, 682-748):
+//               length-m' codelets down the 256 columns x[c + 256 q], then
+//               for column t < 16 and row i0 < m' a 16-point codelet over
+//               b1[256 i0 + t + 16 i] (rows i0 >= 1 twiddled by
+//               W_{16 m'}^{dir i i0}) into b0[16 i0 + t + 16 m' k], then the
+//               twiddled rows of the n = 16 m case over b0.
+// Twiddles are the reference's premultiplied pairs (src/generate_twiddles.hpp:
+// 72-132), passed as short4 (c, s, cvt(-s), c).
+//
+// Saturation: every codelet input is pre-shifted by log2(r), so an interval
+// analysis of each codelet (tests/test_q15.py::test_q15_codelet_
+// intermediates_never_saturate and ::test_q7_codelet_intermediates_never_
+// saturate) shows that only the final output additions can leave B bits and
+// that no MAC lane wraps; intermediates therefore use plain integer
+// arithmetic (identical results) and outputs saturate when packed.
+//
+// GPU mapping: members are staged in shared memory at padded position
+// k + k/16 (a column and a row are both read without bank conflicts).
+// n = 16 m: a CTA takes G members, 16 threads per member run the column
+// codelets in place, then one thread per row runs the twiddled 16-point
+// codelet and stores its outputs.  n = 256 m': one member per CTA of 256
+// threads: one column codelet per thread, one (column, row) task of the
+// inner level per thread, one outer row per thread.
+#include <stdint.h>
+
+#include "kernels.h"
+#include "launch_pdl.cuh"
+#include "ptx.cuh"
+
+namespace plfft_b200 {
+
+struct qc {
+  int re, im;
+};
+
+// lane format: storage word of one complex element and the Q0.(B-1) constants
+template <int B>
+struct Fx;
+template <>
+struct Fx<16> {
+  using W = int;  // int16 (re, im), re in the low half
+  static constexpr int LO = -32768, HI = 32767;
+  static constexpr int C8 = 23170, C16 = 30273, S16 = 12539;  // trunc(2^15 cos/sin)
+};
+template <>
+struct Fx<8> {
+  using W = short;  // int8 (re, im), re in the low byte
+  static constexpr int LO = -128, HI = 127;
+  static constexpr int C8 = 90, C16 = 118, S16 = 48;  // trunc(2^7 cos/sin)
+};
+
+__device__ __forceinline__ int rshr(int v, int s) { return (v + (1 << (s - 1))) >> s; }
+
+template <int B>
+struct Ar {
+  // multiply by a real constant k: never saturates for the operands that
+  // reach it (interval analysis)
+  template <int K>
+  __device__ __forceinline__ static int rdm(int a) {
+    static_assert(K >= Fx<B>::LO && K <= Fx<B>::HI, "constant out of range");
+    return (a * K + (1 << (B - 2))) >> (B - 1);
+  }
+  __device__ __forceinline__ static int mac2(int a, int ka, int b, int kb) {
+    return (a * ka + b * kb + (1 << (B - 2))) >> (B - 1);
+  }
+  __device__ __forceinline__ static qc add(qc a, qc b) { return {a.re + b.re, a.im + b.im}; }
+  __device__ __forceinline__ static qc sub(qc a, qc b) { return {a.re - b.re, a.im - b.im}; }
+  // -1 times a value in range is exact
+  __device__ __forceinline__ static qc mul_pi(qc z) { return {-z.im, rdm<Fx<B>::HI>(z.re)}; }
+  __device__ __forceinline__ static qc mul_mi(qc z) { return {rdm<Fx<B>::HI>(z.im), -z.re}; }
+  __device__ __forceinline__ static qc mul_w8(qc z) {
+    constexpr int C = Fx<B>::C8;
+    return {mac2(z.re, C, rdm<C>(z.im), Fx<B>::HI), mac2(z.im, C, rdm<C>(z.re), Fx<B>::LO)};
+  }
+  __device__ __forceinline__ static qc mul_w8_3(qc z) {
+    constexpr int C = -Fx<B>::C8;
+    return {mac2(z.re, C, rdm<C>(z.im), Fx<B>::LO), mac2(z.im, C, rdm<C>(z.re), Fx<B>::HI)};
+  }
+  __device__ __forceinline__ static qc mul_w(qc z, int wr, int wi) {
+    return {mac2(z.re, wr, z.im, -wi), mac2(z.im, wr, z.re, wi)};
+  }
+  // twiddle (c, s, cvt(-s), c): one rounding per component
+  __device__ __forceinline__ static qc twiddle(qc s, short4 w) {
+    return {mac2(s.re, w.x, s.im, w.z), mac2(s.re, w.y, s.im, w.w)};
+  }
+};
+
+// ---- codelets on pre-scaled inputs, outputs in forward order ----
+template <int B>
+__device__ __forceinline__ void q_dft2(const qc* a, qc* y) {
+  using A = Ar<B>;
+  y[0] = A::add(a[0], a[1]);
+  y[1] = A::sub(a[0], a[1]);
+}
+
+template <int B>
+__device__ __forceinline__ void q_dft4(const qc* a, qc* y) {
+  using A = Ar<B>;
+  const qc s02 = A::add(a[0], a[2]), s13 = A::add(a[1], a[3]);
+  const qc d02 = A::sub(a[0], a[2]), j13 = A::mul_pi(A::sub(a[1], a[3]));
+  y[0] = A::add(s02, s13);
+  y[2] = A::sub(s02, s13);
+  y[1] = A::sub(d02, j13);
+  y[3] = A::add(d02, j13);
+}
+
+template <int B>
+__device__ __forceinline__ void q_dft8(const qc* a, qc* y) {
+  using A = Ar<B>;
+  constexpr int C8 = Fx<B>::C8, HI = Fx<B>::HI, LO = Fx<B>::LO;
+  qc p[4], m[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    p[k] = A::add(a[k], a[k + 4]);
+    m[k] = A::sub(a[k], a[k + 4]);
+  }
+  const qc e0 = A::add(p[0], p[2]), e1 = A::add(p[1], p[3]);
+  y[0] = A::add(e0, e1);
+  y[4] = A::sub(e0, e1);
+  const qc d = A::sub(p[0], p[2]), jd = A::mul_pi(A::sub(p[1], p[3]));
+  y[2] = A::sub(d, jd);
+  y[6] = A::add(d, jd);
+  const qc z = A::add(m[1], m[3]), w = A::sub(m[1], m[3]);
+  const qc rd = {A::template rdm<C8>(w.re), A::template rdm<C8>(w.im)};
+  const qc x = {A::mac2(m[2].im, LO, z.im, -C8), A::mac2(m[2].re, HI, z.re, C8)};
+  const qc x2 = {A::mac2(m[2].im, LO, z.im, C8), A::mac2(m[2].re, HI, z.re, -C8)};
+  const qc u = A::add(m[0], rd), v = A::sub(m[0], rd);
+  y[1] = A::sub(u, x);
+  y[7] = A::add(u, x);
+  y[3] = A::add(v, x2);
+  y[5] = A::sub(v, x2);
+}
+
+template <int B>
+__device__ __forceinline__ void q_dft16(const qc* a, qc* y) {
+  using A = Ar<B>;
+  constexpr int C16 = Fx<B>::C16, S16 = Fx<B>::S16;
+  qc p[8], m[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    p[k] = A::add(a[k], a[k + 8]);
+    m[k] = A::sub(a[k], a[k + 8]);
+  }
+  const qc s04 = A::add(p[0], p[4]), s26 = A::add(p[2], p[6]);
+  const qc s15 = A::add(p[1], p[5]), s37 = A::add(p[3], p[7]);
+  const qc e0 = A::add(s04, s26), e1 = A::add(s15, s37);
+  y[0] = A::add(e0, e1);
+  y[8] = A::sub(e0, e1);
+  const qc Aq = A::sub(s04, s26), jB = A::mul_pi(A::sub(s15, s37));
+  y[4] = A::sub(Aq, jB);
+  y[12] = A::add(Aq, jB);
+  const qc C = A::sub(p[0], p[4]), jD = A::mul_pi(A::sub(p[2], p[6]));
+  const qc kE = A::mul_w8(A::sub(p[1], p[5])), kF = A::mul_w8_3(A::sub(p[3], p[7]));
+  const qc g1 = A::sub(C, jD), g2 = A::add(C, jD);
+  const qc h = A::add(kE, kF), h2 = A::mul_mi(A::sub(kF, kE));
+  y[2] = A::add(g1, h);
+  y[10] = A::sub(g1, h);
+  y[6] = A::sub(g2, h2);
+  y[14] = A::add(g2, h2);
+  const qc j4 = A::mul_pi(m[4]);
+  const qc q = A::sub(m[0], j4), q2 = A::add(m[0], j4);
+  const qc k2 = A::mul_w8(m[2]), k6 = A::mul_w8_3(m[6]);
+  const qc r = A::add(k2, k6), r2 = A::mul_mi(A::sub(k6, k2));
+  const qc j5 = A::mul_pi(m[5]), j7 = A::mul_pi(m[7]);
+  const qc u = A::sub(m[1], j5), u2 = A::add(m[1], j5);
+  const qc v = A::sub(m[3], j7), v2 = A::add(m[3], j7);
+  const qc l1 = A::mul_w(u, C16, -S16), l3 = A::mul_w(v, S16, -C16);
+  const qc l3b = A::mul_w(u2, S16, -C16), l9 = A::mul_w(v2, -C16, S16);
+  const qc qr = A::add(q, r), qmr = A::sub(q, r);
+  const qc ls = A::add(l1, l3), ld = A::mul_mi(A::sub(l3, l1));
+  y[1] = A::add(qr, ls);
+  y[9] = A::sub(qr, ls);
+  y[5] = A::sub(qmr, ld);
+  y[13] = A::add(qmr, ld);
+  const qc qa = A::sub(q2, r2), qb = A::add(q2, r2);
+  const qc ls2 = A::add(l3b, l9), ld2 = A::mul_mi(A::sub(l9, l3b));
+  y[3] = A::add(qa, ls2);
+  y[11] = A::sub(qa, ls2);
+  y[7] = A::sub(qb, ld2);
+  y[15] = A::add(qb, ld2);
+}
+
+template <int R, int B>
+__device__ __forceinline__ void q_dft(const qc* a, qc* y) {
+  if constexpr (R == 1)
+    y[0] = a[0];
+  else if constexpr (R == 2)
+    q_dft2<B>(a, y);
+  else if constexpr (R == 4)
+    q_dft4<B>(a, y);
+  else if constexpr (R == 8)
+    q_dft8<B>(a, y);
+  else
+    q_dft16<B>(a, y);
+}
+
+constexpr int ilog2_c(int r) { return r <= 1 ? 0 : 1 + ilog2_c(r / 2); }
+
+// storage word <-> components (little endian: re in the low part)
+__device__ __forceinline__ qc unpack(int w) { return {(w << 16) >> 16, w >> 16}; }
+__device__ __forceinline__ qc unpack(short w) {
+  const int v = w;
+  return {(v << 24) >> 24, v >> 8};
+}
+// saturate both components to B bits and pack
+template <int B>
+__device__ __forceinline__ typename Fx<B>::W pack(qc v) {
+  if constexpr (B == 16) {
+    int d;
+    asm("cvt.pack.sat.s16.s32 %0, %1, %2;" : "=r"(d) : "r"(v.im), "r"(v.re));
+    return d;
+  } else {
+    const int re = max(-128, min(127, v.re)), im = max(-128, min(127, v.im));
+    return short((re & 0xff) | (im << 8));
+  }
+}
+
+template <int B>
+__device__ __forceinline__ qc pre(qc v, int s) {
+  return {rshr(v.re, s), rshr(v.im, s)};
+}
+
+// n <= 16: one thread per member
+template <int N, int DIR, int B>
+__global__ void __launch_bounds__(256) fx_small_kernel(const FixedLaunch L) {
+  using W = typename Fx<B>::W;
+  griddep_wait();  // launched programmatically (launch_pdl.cuh)
+  griddep_launch_dependents();
+  const int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b >= L.howmany) return;
+  constexpr int S = ilog2_c(N);
+  const W* x = static_cast<const W*>(L.in) + b * L.idist;
+  W* y = static_cast<W*>(L.out) + b * L.odist;
+  qc a[N], r[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    const qc v = unpack(x[k * L.istride]);
+    a[k] = S ? pre<B>(v, S) : v;
+  }
+  q_dft<N, B>(a, r);
+#pragma unroll
+  for (int k = 0; k < N; ++k) y[k * L.ostride] = pack<B>(r[DIR < 0 ? k : (N - k) % N]);
+}
+
+// padded shared-memory position of element k (16 columns per row, one
+// spare word per row) and the member pitch (== 16 mod 32 words)
+__host__ __device__ constexpr int fx_pos(int k) { return k + (k >> 4); }
+__host__ __device__ constexpr int fx_pitch(int n) { return ((17 * (n / 16) + 15) / 32) * 32 + 16; }
+
+// n = 16 m, m = 2..16: G = blockDim / 16 members per CTA
+template <int N, int DIR, int B>
+__global__ void __launch_bounds__(256) fx_two_stage_kernel(const FixedLaunch L) {
+  using W = typename Fx<B>::W;
+  griddep_wait();  // launched programmatically (launch_pdl.cuh)
+  griddep_launch_dependents();
+  constexpr int M = N / 16, SM = ilog2_c(M);
+  constexpr int PITCH = fx_pitch(N);
+  extern __shared__ __align__(16) unsigned char fsm[];
+  short4* tw = reinterpret_cast<short4*>(fsm);  // (c, s, cvt(-s), c)
+  W* tile = reinterpret_cast<W*>(tw + 15 * (M - 1 > 0 ? M - 1 : 1));
+  const int G = blockDim.x / 16;
+  const int64_t b0 = int64_t(blockIdx.x) * G;
+  const int64_t left = L.howmany - b0;
+  const int cnt = left < G ? int(left) : G;
+  for (int i = threadIdx.x; i < 15 * (M - 1); i += blockDim.x) tw[i] = L.tw[i];
+  const W* in = static_cast<const W*>(L.in);
+  // stage the members (each thread: consecutive elements across members),
+  // asynchronous copies so that all of a thread's loads are in flight
+  for (int f = threadIdx.x; f < cnt * N; f += blockDim.x) {
+    const int g = f / N, k = f - g * N;
+    const W* src = in + (b0 + g) * L.idist + int64_t(k) * L.istride;
+    if constexpr (B == 16)
+      cp_async4(tile + g * PITCH + fx_pos(k), src);
+    else
+      tile[g * PITCH + fx_pos(k)] = *src;
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const int g = threadIdx.x >> 4, c = threadIdx.x & 15;
+  W* mine = tile + g * PITCH;
+  if (g < cnt) {  // stage 1: length-M codelet down column c, in place
+    qc a[M], r[M];
+#pragma unroll
+    for (int q = 0; q < M; ++q) a[q] = pre<B>(unpack(mine[fx_pos(c + 16 * q)]), SM);
+    q_dft<M, B>(a, r);
+#pragma unroll
+    for (int k = 0; k < M; ++k) mine[fx_pos(c + 16 * k)] = pack<B>(r[DIR < 0 ? k : (M - k) % M]);
+  }
+  __syncthreads();
+  // stage 2: rows (member, j) spread over the CTA's threads
+  for (int row = threadIdx.x; row < cnt * M; row += blockDim.x) {
+    const int gg = row / M, j = row - gg * M;
+    const W* src = tile + gg * PITCH + fx_pos(16 * j);
+    qc a[16], r[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const qc s = pre<B>(unpack(src[i]), 4);
+      a[i] = (i == 0 || j == 0) ? s : Ar<B>::twiddle(s, tw[15 * (j - 1) + (i - 1)]);
+    }
+    q_dft<16, B>(a, r);
+    W* y = static_cast<W*>(L.out) + (b0 + gg) * L.odist;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) y[int64_t(j + M * k) * L.ostride] = pack<B>(r[DIR < 0 ? k : (16 - k) & 15]);
+  }
+}
+
+// n = 256 m', m' = 2..16: one member per CTA of 256 threads
+template <int N, int DIR, int B>
+__global__ void __launch_bounds__(256) fx_three_stage_kernel(const FixedLaunch L) {
+  using W = typename Fx<B>::W;
+  griddep_wait();  // launched programmatically (launch_pdl.cuh)
+  griddep_launch_dependents();
+  constexpr int M2 = N / 256, S2 = ilog2_c(M2), M = N / 16;
+  extern __shared__ __align__(16) unsigned char fsm[];
+  W* t = reinterpret_cast<W*>(fsm);
+  const int64_t b = blockIdx.x;
+  const W* x = static_cast<const W*>(L.in) + b * L.idist;
+  W* y = static_cast<W*>(L.out) + b * L.odist;
+  for (int k = threadIdx.x; k < N; k += 256) t[fx_pos(k)] = x[int64_t(k) * L.istride];
+  __syncthreads();
+  {  // length-M2 codelet down column c = threadIdx.x, in place
+    const int c = threadIdx.x;
+    qc a[M2], r[M2];
+#pragma unroll
+    for (int q = 0; q < M2; ++q) a[q] = pre<B>(unpack(t[fx_pos(c + 256 * q)]), S2);
+    q_dft<M2, B>(a, r);
+#pragma unroll
+    for (int k = 0; k < M2; ++k) t[fx_pos(c + 256 * k)] = pack<B>(r[DIR < 0 ? k : (M2 - k) % M2]);
+  }
+  __syncthreads();
+  // inner radix-16 level: task (row i0, column tc)
+  const int i0 = threadIdx.x >> 4, tc = threadIdx.x & 15;
+  const bool act = threadIdx.x < 16 * M2;
+  qc r[16];
+  if (act) {
+    qc a[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const qc s = pre<B>(unpack(t[fx_pos(256 * i0 + tc + 16 * i)]), 4);
+      a[i] = (i == 0 || i0 == 0) ? s : Ar<B>::twiddle(s, __ldg(L.tw2 + 15 * (i0 - 1) + (i - 1)));
+    }
+    q_dft<16, B>(a, r);
+  }
+  __syncthreads();  // every input of this level is read before any output lands
+  if (act) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) t[fx_pos(16 * i0 + tc + 16 * M2 * k)] = pack<B>(r[DIR < 0 ? k : (16 - k) & 15]);
+  }
+  __syncthreads();
+  // outer radix-16 level: row j
+  if (threadIdx.x < M) {
+    const int j = threadIdx.x;
+    qc a[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const qc s = pre<B>(unpack(t[fx_pos(16 * j + i)]), 4);
+      a[i] = (i == 0 || j == 0) ? s : Ar<B>::twiddle(s, __ldg(L.tw + 15 * (j - 1) + (i - 1)));
+    }
+    q_dft<16, B>(a, r);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) y[int64_t(j + M * k) * L.ostride] = pack<B>(r[DIR < 0 ? k : (16 - k) & 15]);
+  }
+}
+
+bool fixed_supported(int64_t n) { return n >= 1 && n <= 4096 && (n & (n - 1)) == 0; }
+
+template <int B>
+static int fx_smem_bytes(int n, int members) {
+  using W = typename Fx<B>::W;
+  if (n <= 16) return 0;
+  if (n > 256) return int(sizeof(W)) * (n + n / 16);
+  return 8 * 15 * (n / 16 - 1 > 0 ? n / 16 - 1 : 1) + int(sizeof(W)) * members * fx_pitch(n);
+}
+
+template <int N, int DIR, int B>
+static cudaError_t run_fx(const FixedLaunch& L, cudaStream_t st) {
+  if constexpr (N <= 16) {
+    const int64_t blocks = (L.howmany + 255) / 256;
+    return launch_pdl(fx_small_kernel<N, DIR, B>, dim3(unsigned(blocks)), dim3(256), 0, st, L);
+  } else if constexpr (N <= 256) {
+    constexpr int kThreads = 256, G = kThreads / 16;
+    const int smem = fx_smem_bytes<B>(N, G);
+    const int64_t blocks = (L.howmany + G - 1) / G;
+    return launch_pdl(fx_two_stage_kernel<N, DIR, B>, dim3(unsigned(blocks)), dim3(kThreads), size_t(smem), st, L);
+  } else {
+    const int smem = fx_smem_bytes<B>(N, 1);
+    return launch_pdl(fx_three_stage_kernel<N, DIR, B>, dim3(unsigned(L.howmany)), dim3(256), size_t(smem), st, L);
+  }
+}
+
+template <int B>
+static cudaError_t launch_fx(int n, int dir, const FixedLaunch& L, cudaStream_t st) {
+#define PLFFT_B200_FX(NV) \
+  if (n == NV) return dir < 0 ? run_fx<NV, -1, B>(L, st) : run_fx<NV, 1, B>(L, st);
+  PLFFT_B200_FX(1)
+  PLFFT_B200_FX(2)
+  PLFFT_B200_FX(4)
+  PLFFT_B200_FX(8)
+  PLFFT_B200_FX(16)
+  PLFFT_B200_FX(32)
+  PLFFT_B200_FX(64)
+  PLFFT_B200_FX(128)
+  PLFFT_B200_FX(256)
+  PLFFT_B200_FX(512)
+  PLFFT_B200_FX(1024)
+  PLFFT_B200_FX(2048)
+  PLFFT_B200_FX(4096)
+#undef PLFFT_B200_FX
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_fixed(int bits, int n, int dir, const FixedLaunch& L, cudaStream_t st) {
+  if (L.howmany > 0x7fffffffLL && n > 256) return cudaErrorInvalidValue;  // one CTA per member
+  return bits == 16 ? launch_fx<16>(n, dir, L, st) : launch_fx<8>(n, dir, L, st);
+}
+
+}  // namespace plfft_b200

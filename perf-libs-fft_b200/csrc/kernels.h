@@ -233,17 +233,19 @@ int fourstep_pass_e(int nl);
 int fourstep_pass_smem(int nl, int c);
 cudaError_t launch_fourstep_pass(int nl, int dir, const FourStepLaunch& L, cudaStream_t st);
 
-// Q0.15 fixed-point C2C (q15.cu): power-of-two n <= 256; elements are
-// int16 (re, im) pairs handled as one 32-bit word; strides in elements.
-struct Q15Launch {
-  const int* in;
-  int* out;
+// Fixed-point C2C (fixed_point.cu), Q0.15 (bits 16) and Q0.7 (bits 8):
+// power-of-two n <= 4096; one complex element is one storage word (int32
+// for two int16, int16 for two int8); strides in elements.
+struct FixedLaunch {
+  const void* in;
+  void* out;
   int64_t howmany;
   int64_t istride, idist, ostride, odist;
-  const int2* tw;  // n >= 32: per row j >= 1 and input i >= 1, words (c, s) and (-s, c)
+  const short4* tw;   // n >= 32: outer radix-16 level, per row j >= 1 and input i >= 1: (c, s, cvt(-s), c)
+  const short4* tw2;  // n >= 512: inner radix-16 level over n / 256 rows, same layout
 };
-bool q15_supported(int64_t n);
-cudaError_t launch_q15(int n, int dir, const Q15Launch& L, cudaStream_t st);
+bool fixed_supported(int64_t n);
+cudaError_t launch_fixed(int bits, int n, int dir, const FixedLaunch& L, cudaStream_t st);
 
 // Split-BF16 tensor-core pass (split_bf16.cu): same addressing as a
 // four-step pass, on-chip length nl in {256, 4096} as radix-16 DFT-matrix

@@ -172,8 +172,9 @@ std::unique_ptr<Node> autotune_c2c(const ConfigData& c, const Layout& lay, std::
 std::unique_ptr<Node> make_fp64_node(int kind, int64_t n, const Layout& lay, int dir, double scale,
                                      std::string* why);
 
-// Q0.15 fixed-point C2C node (plan_q15.cpp); nullptr (with why) if unsupported.
-std::unique_ptr<Node> make_q15_node(int64_t n, const Layout& lay, int dir, std::string* why);
+// Fixed-point C2C node (plan_fixed.cpp), bits 16 (Q0.15) or 8 (Q0.7);
+// nullptr (with why) if unsupported.
+std::unique_ptr<Node> make_fixed_node(int bits, int64_t n, const Layout& lay, int dir, std::string* why);
 
 // FP64 host helpers for table generation (plan_conv.cpp)
 using cd = std::complex<double>;

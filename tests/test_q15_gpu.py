@@ -9,7 +9,7 @@ import oracle
 
 pytestmark = pytest.mark.gpu
 
-SIZES = [1, 2, 4, 8, 16, 32, 64, 128, 256]
+SIZES = [1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096]
 
 
 def _device_q15(n, buf_in, howmany, direction, istride=1, idist=None, ostride=1, odist=None, out_words=None,
@@ -57,7 +57,7 @@ def test_q15_random_batches_bit_exact(n, direction):
     assert np.array_equal(out.view(np.int16).reshape(x.shape), ref), plan.describe()
 
 
-@pytest.mark.parametrize("n", [4, 16, 256])
+@pytest.mark.parametrize("n", [4, 16, 256, 1024])
 def test_q15_strided_layouts_and_guard_words(n):
     """Interleaved members (idist = 1, istride = howmany) in; strided out with
     gaps whose words must stay untouched."""
@@ -83,7 +83,7 @@ def test_q15_strided_layouts_and_guard_words(n):
     assert np.all(got[mask] == sentinel)
 
 
-@pytest.mark.parametrize("n", [8, 128])
+@pytest.mark.parametrize("n", [8, 128, 2048])
 def test_q15_in_place(n):
     rng = np.random.default_rng(9)
     hm = 77
@@ -95,7 +95,7 @@ def test_q15_in_place(n):
 def test_q15_unsupported_configs_fail_plan_creation():
     import plfft
 
-    for kw in ({"n": 512}, {"n": 24}):
+    for kw in ({"n": 8192}, {"n": 24}):
         with pytest.raises(plfft.PlfftError) as e:
             plfft.make_plan("c2c", kw["n"], 4, data_type=plfft.DataType.Q15)
         assert e.value.status == plfft.Status.PLAN_CREATION_FAILED
