@@ -68,7 +68,7 @@ def test_q7_reference_strided_layouts_and_guard_words(case):
     idx_i = np.arange(hm)[:, None] * id_ + np.arange(n)[None, :] * is_
     buf[idx_i] = xs
     total = (hm - 1) * od + (n - 1) * os_ + 1 + 8
-    sentinel = np.int16(0x5AA5 - 0x10000)
+    sentinel = np.int16(0x5AA5)
     out, plan = _device_q7(n, buf, hm, -1, is_, id_, os_, od, out_elems=total, fill=int(sentinel))
     idx_o = np.arange(hm)[:, None] * od + np.arange(n)[None, :] * os_
     ref = oracle.q7_c2c(xs, -1).view(np.int16).reshape(hm, n)
