@@ -63,15 +63,28 @@ __device__ __forceinline__ void st_bfly(float2 (&v)[E], int t, const float2* __r
   }
 }
 
+// Exchange padding: one spare complex every 2^PS.  A stage's scatter
+// writes, for a fixed output i, the 16 threads of a half-warp to addresses
+// R (j / NS) NS + j mod NS + i NS: with one spare every 16 complex, radix
+// <= 16 rows land on 16 distinct 8-byte bank pairs, but radix-32 rows (a
+// stride of 34) collide two ways; one spare every 32 (a stride of 33)
+// separates them.  Each exchange picks its own padding (the gather that
+// follows uses the same), sized within spad_len().
+template <int R>
+constexpr int exchange_pad_shift() { return R >= 32 ? 5 : 4; }
+template <int PS>
+__device__ __forceinline__ int xpad(int p) { return p + (p >> PS); }
+
 template <int T, int E, int R, int NS>
 __device__ __forceinline__ void st_scatter(const float2 (&v)[E], int t, float2* sm) {
   constexpr int M = E / R;
+  constexpr int PS = exchange_pad_shift<R>();
 #pragma unroll
   for (int m = 0; m < M; ++m) {
     const int j = t + T * m;
     const int base = (j & ~(NS - 1)) * R + (j & (NS - 1));
 #pragma unroll
-    for (int i = 0; i < R; ++i) sm[spad(base + i * NS)] = v[m + M * i];
+    for (int i = 0; i < R; ++i) sm[xpad<PS>(base + i * NS)] = v[m + M * i];
   }
 }
 
@@ -84,8 +97,9 @@ struct Stages {
       sync();  // the buffer's previous contents are fully read
       st_scatter<P::T, E, P::radix(S - 1), P::ns(S - 1)>(v, t, xb);
       sync();
+      constexpr int PS = exchange_pad_shift<P::radix(S - 1)>();
 #pragma unroll
-      for (int q = 0; q < E; ++q) v[q] = xb[spad(t + P::T * q)];
+      for (int q = 0; q < E; ++q) v[q] = xb[xpad<PS>(t + P::T * q)];
       st_bfly<P::T, E, P::radix(S), P::ns(S), P::twoff(S), DIR, TWS, RMIN>(v, t, tw);
       Stages<N, E, DIR, S + 1, TWS, RMIN>::run(v, t, xb, tw, sync);
     }
