@@ -373,7 +373,7 @@ class GroupedWorkload(Workload):
 
     desc = ("grouped C2C FP32: 4000 transforms, log-uniform 16..65536 (60% pow2, 20% 2^a3^b5^c7^d, "
             "10% Rader primes, 10% Bluestein)")
-    profile = None
+    profile = "grouped_4000"
 
     def __init__(self, count=4000, per_length=False):
         import numpy as np
@@ -548,7 +548,7 @@ class AdjointWorkload(PlanWorkload):
 
     def __init__(self):
         super().__init__("diff_r2c_n8192_b1024", "loss = sum W |R2C(x)|^2 forward + adjoint, N=8192 batch=1024",
-                         "r2c", 8192, 1024)
+                         "r2c", 8192, 1024, profile="real_fused_diff_n8192_b1024")
 
     def algo_bytes(self):
         n, b = self.n, self.batch
@@ -612,7 +612,7 @@ class Q15Workload(PlanWorkload):
     data = "synthetic (seeded int16 re/im uniform in [-2^14, 2^14))"
 
     def __init__(self, name, desc, n, batch):
-        super().__init__(name, desc, "c2c", n, batch, profile="q15_two_stage_n256_b16384")
+        super().__init__(name, desc, "c2c", n, batch, profile="fx_two_stage_q15_n256_b16384")
 
     def sizes(self):
         return self.n * self.batch * 4, self.n * self.batch * 4
@@ -688,12 +688,15 @@ def make_workload(name):
         "dct2_n1024_b4096": lambda: PlanWorkload("dct2_n1024_b4096", "R2R DCT-II FP32 N=1024 batch=4096", "r2r",
                                                  1024, 4096, r2r="DCT_2", profile="real_fused_dct2_n1024_b4096"),
         "dst2_n1024_b4096": lambda: PlanWorkload("dst2_n1024_b4096", "R2R DST-II FP32 N=1024 batch=4096", "r2r",
-                                                 1024, 4096, r2r="DST_2"),
-        "c2c_n1m_b64": lambda: PlanWorkload("c2c_n1m_b64", "C2C FP32 N=2^20 batch=64", "c2c", 1 << 20, 64),
-        "c2c_n64k_b1024": lambda: PlanWorkload("c2c_n64k_b1024", "C2C FP32 N=2^16 batch=1024", "c2c", 1 << 16, 1024),
+                                                 1024, 4096, r2r="DST_2", profile="real_fused_dst2_n1024_b4096"),
+        "c2c_n1m_b64": lambda: PlanWorkload("c2c_n1m_b64", "C2C FP32 N=2^20 batch=64", "c2c", 1 << 20, 64,
+                                            profile="fourstep_pass_n1m_b64"),
+        "c2c_n64k_b1024": lambda: PlanWorkload("c2c_n64k_b1024", "C2C FP32 N=2^16 batch=1024", "c2c", 1 << 16, 1024,
+                                               profile="fourstep_pass_n64k_b1024"),
         "c2c_n1m_b64_split_bf16": lambda: PlanWorkload("c2c_n1m_b64_split_bf16",
                                                        "C2C N=2^20 batch=64, split-BF16 tensor-core stages",
-                                                       "c2c", 1 << 20, 64, precision=1),
+                                                       "c2c", 1 << 20, 64, precision=1,
+                                                       profile="split_bf16_pass_n1m_b64"),
         "c2c_n64k_b1024_split_bf16": lambda: PlanWorkload("c2c_n64k_b1024_split_bf16",
                                                           "C2C N=2^16 batch=1024, split-BF16 tensor-core stages",
                                                           "c2c", 1 << 16, 1024, precision=1,
@@ -702,6 +705,16 @@ def make_workload(name):
         "grouped_4000_per_length": lambda: GroupedWorkload(per_length=True),
         "q15_n256_b16384": lambda: Q15Workload("q15_n256_b16384", "C2C Q0.15 forward N=256 batch=16384", 256, 16384),
         "diff_r2c_n8192_b1024": lambda: AdjointWorkload(),
+        # kernel-coverage workloads (not benchmark configurations): the
+        # smooth non-power-of-two, Rader, Bluestein and real-wrap schedules
+        "c2c_n1000_b16384": lambda: PlanWorkload("c2c_n1000_b16384", "C2C FP32 N=1000 (2^3 5^3) batch=16384",
+                                                 "c2c", 1000, 16384, profile="c2c_reg_n1000_b16384"),
+        "c2c_n1009_b8192": lambda: PlanWorkload("c2c_n1009_b8192", "C2C FP32 N=1009 (Rader) batch=8192",
+                                                "c2c", 1009, 8192, profile="conv_rader_n1009_b8192"),
+        "c2c_n1031_b8192": lambda: PlanWorkload("c2c_n1031_b8192", "C2C FP32 N=1031 (Bluestein) batch=8192",
+                                                "c2c", 1031, 8192, profile="conv_bluestein_n1031_b8192"),
+        "r2c_n1000_b16384": lambda: PlanWorkload("r2c_n1000_b16384", "R2C FP32 N=1000 (real wrap) batch=16384",
+                                                 "r2c", 1000, 16384, profile="realwrap_r2c_n1000_b16384"),
     }
     return table[name]()
 
@@ -709,7 +722,8 @@ def make_workload(name):
 WORKLOAD_NAMES = ["c2c_n1024_b4096", "r2c_c2r_n4096_b8192", "dct2_n1024_b4096", "dst2_n1024_b4096", "c2c_n1m_b64",
                   "c2c_n64k_b1024", "c2c_n1m_b64_split_bf16", "c2c_n64k_b1024_split_bf16", "grouped_4000",
                   "grouped_4000_per_length",
-                  "diff_r2c_n8192_b1024", "q15_n256_b16384"]
+                  "diff_r2c_n8192_b1024", "q15_n256_b16384",
+                  "c2c_n1000_b16384", "c2c_n1009_b8192", "c2c_n1031_b8192", "r2c_n1000_b16384"]
 
 
 # --------------------------------------------------------------------------
@@ -724,13 +738,15 @@ def peaks():
 
 
 def profile_traffic(name):
-    """dram bytes per launch of the dominant kernel from the committed ncu summary."""
+    """Steady-state DRAM bytes (read + write) of one step from the committed
+    ncu summary: all of the step's kernels, three consecutive steps captured
+    without cache flushing, averaged."""
     if not name:
         return None
     path = os.path.join(ROOT, "profiles", name + ".md")
     if not os.path.exists(path):
         return None
-    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+    m = re.search(r"traffic_bytes_per_step:\s*([0-9.eE+]+)", open(path).read())
     return float(m.group(1)) if m else None
 
 
