@@ -1,6 +1,6 @@
 """Generate reference-output fixtures by executing the reference's own NEON
 kernels (interpreter: neon_a64.py) composed as its ESTIMATE plans
-(ref_c2c_plan.py).
+(ref_plan.py).
 
 Run once, in a container that holds the reference sources:
     python tests/golden/make_ref_golden.py <path to the reference checkout> [q15 q7 f32]
@@ -16,6 +16,13 @@ Writes:
   f32_c2c_reference.npz  FP32 C2C for a spread of lengths (single-radix,
                          two-level and three-level plans), both directions,
                          4 members of U[-1, 1) data
+  f32_real_reference.npz FP32 R2C and C2R for the same kind of spread, and
+                         DCT-II / DST-II: the reference's R2R plan is, per
+                         member, an input permutation, its ESTIMATE R2C plan
+                         of length n, and a post-rotation
+                         (r2r_plan.cpp:56-77, r2r_buffer_helper.hpp:316-335,
+                         455-469, 686-701, 828-854); the permutation and
+                         rotation are restated here in single precision
 """
 import os
 import sys
@@ -25,7 +32,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 import neon_a64  # noqa: E402
-import ref_c2c_plan  # noqa: E402
+import ref_plan  # noqa: E402
 
 FIXED_SOURCES = {
     "q15": ["plfft_q15_jjjn_uu.S", "plfft_q15_jjjn_uun.S", "plfft_q15_jjjn_gs.S", "plfft_q15_jjjn_gu.S",
@@ -40,6 +47,16 @@ F32_SOURCES = ["plfft_cccn_uu.S", "plfft_cccn_uun.S", "plfft_cccn_gs.S", "plfft_
 
 FIXED_SIZES = [2, 4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096]
 F32_SIZES = [2, 3, 5, 7, 8, 12, 16, 20, 32, 64, 100, 128, 360, 1000, 1024, 4096]
+REAL_SIZES = [2, 3, 8, 16, 20, 64, 100, 256, 1000, 1024, 4096]
+R2R_SIZES = [16, 100, 1024]
+REAL_SOURCES = F32_SOURCES + ["plfft_sccnoh_uu.S", "plfft_sccnoh_uun.S", "plfft_sccnoh_gs.S", "plfft_sccnoh_gu.S",
+                              "plfft_sccnoh_us.S", "plfft_ccsn_uu.S", "plfft_ccsn_uun.S", "plfft_ccsn_gs.S",
+                              "plfft_ccsn_gu.S", "plfft_ccsn_us.S", "plfft_cccnoh_uu.S", "plfft_cccnoh_uun.S",
+                              "plfft_cccnih_uu.S", "plfft_cccnih_uun.S", "plfft_ab_ccctj_dit_gu.S",
+                              "plfft_ab_ccctj_dit_gs.S", "plfft_ab_ccctol_dit_uun.S", "plfft_ab_ccctil_dif_us.S",
+                              "plfft_ab_ccctil_dif_gs.S", "plfft_ab_ccctih_dif_us.S", "plfft_ab_ccctih_dif_gs.S",
+                              "plfft_ac_ccctj_dit_uu.S", "plfft_ac_ccctol_dit_uu.S", "plfft_ac_ccctil_dif_uu.S",
+                              "plfft_ac_ccctih_dif_uu.S"]
 
 
 def fixed_inputs(n, seed, bits):
@@ -64,7 +81,7 @@ def run(kern, dtype, n, dirn, x):
     machine = neon_a64.Machine(kern)
     hm = x.shape[0]
     flat = x.reshape(-1) if dtype == "f32" else x.reshape(-1, 2)
-    y, desc = ref_c2c_plan.run_c2c(machine, dtype, dirn, flat, n, hm)
+    y, desc = ref_plan.run_c2c(machine, dtype, dirn, flat, n, hm)
     return y.reshape(x.shape), desc
 
 
@@ -98,15 +115,90 @@ def make_f32(kdir):
     np.savez_compressed(os.path.join(HERE, "f32_c2c_reference.npz"), **out)
 
 
+def dct2_input(x):
+    """r2r_buffer_helper<DCT_2>::prepare_fft_input: even elements to the
+    first half, odd elements reversed into the second half."""
+    n = x.shape[-1]
+    i = np.arange(n)
+    src = np.where(i < (n + 1) // 2, 2 * i, 2 * (n - i) - 1)
+    return x[..., src]
+
+
+def dst2_input(x):
+    """r2r_buffer_helper<DST_2>::prepare_fft_input: fft_in[j] = +-x[i],
+    j = i / 2 (i even), n - (i + 1) / 2 (i odd, negated)."""
+    n = x.shape[-1]
+    out = np.empty_like(x)
+    for i in range(n):
+        j = n - (i + 1) // 2 if i % 2 else i // 2
+        out[..., j] = -x[..., i] if i % 2 else x[..., i]
+    return out
+
+
+def dct2_output(F, n):
+    """r2r_buffer_helper<DCT_2>::extract_output_from_fft with the single-
+    precision rotation w_k = (cos m, -sin m), m = pi k / 2n
+    (generate_twiddles.hpp:191-194)."""
+    y = np.empty(F.shape[:-1] + (n,), np.float32)
+    y[..., 0] = F[..., 0].real * np.float32(2)
+    for k in range(1, n // 2 + 1):
+        m = np.float32(np.pi) * np.float32(k) / np.float32(2 * n)
+        w = np.complex64(complex(np.cos(m), -np.sin(m)))
+        j = (F[..., k] * w) * np.complex64(2)
+        y[..., k] = j.real
+        y[..., n - k] = -j.imag
+    return y
+
+
+def dst2_output(F, n):
+    """r2r_buffer_helper<DST_2>::extract_output_from_fft: division by
+    (sin c, -cos c), c = pi i / 2n, real part times 2."""
+    y = np.empty(F.shape[:-1] + (n,), np.float32)
+    h = n // 2 + 1
+    for i in range(1, n):
+        tmp = F[..., i] if i < h else np.conj(F[..., n - i])
+        c = np.float32(0.5 * np.pi * i / n)
+        d = complex(np.sin(c), -np.cos(c))
+        y[..., i - 1] = (tmp.astype(np.complex128) / d).real.astype(np.float32) * np.float32(2)
+    y[..., n - 1] = F[..., 0].real * np.float32(2)
+    return y
+
+
+def make_real(kdir):
+    kern = neon_a64.Kernels([os.path.join(kdir, s) for s in REAL_SOURCES])
+    out = {}
+    for n in REAL_SIZES:
+        rng = np.random.default_rng(6000 + n)
+        h = n // 2 + 1
+        x = rng.uniform(-1, 1, (4, n)).astype(np.float32)
+        y, desc = ref_plan.run(neon_a64.Machine(kern), "f32", "r2c", -1, x.ravel(), n, 4)
+        out[f"r2c_x_{n}"], out[f"r2c_y_{n}"], out[f"r2c_plan_{n}"] = x, y.reshape(4, h), np.array(desc)
+        X = (rng.uniform(-1, 1, (4, h)) + 1j * rng.uniform(-1, 1, (4, h))).astype(np.complex64)
+        y, desc = ref_plan.run(neon_a64.Machine(kern), "f32", "c2r", 1, X.ravel(), n, 4)
+        out[f"c2r_x_{n}"], out[f"c2r_y_{n}"], out[f"c2r_plan_{n}"] = X, y.reshape(4, n), np.array(desc)
+        print("f32 real", n, desc, flush=True)
+    for n in R2R_SIZES:
+        rng = np.random.default_rng(6500 + n)
+        x = rng.uniform(-1, 1, (4, n)).astype(np.float32)
+        for name, pre, post in (("dct2", dct2_input, dct2_output), ("dst2", dst2_input, dst2_output)):
+            F = np.stack([ref_plan.run(neon_a64.Machine(kern), "f32", "r2c", -1, pre(x[b]), n, 1)[0]
+                          for b in range(4)])
+            out[f"{name}_x_{n}"], out[f"{name}_y_{n}"] = x, post(F, n)
+        print("f32 r2r", n, flush=True)
+    np.savez_compressed(os.path.join(HERE, "f32_real_reference.npz"), **out)
+
+
 def main():
     kdir = os.path.join(sys.argv[1], "src", "providers", "aot", "asm", "neon")
-    which = sys.argv[2:] or ["q15", "q7", "f32"]
+    which = sys.argv[2:] or ["q15", "q7", "f32", "real"]
     if "q15" in which:
         make_fixed(kdir, "q15", 16)
     if "q7" in which:
         make_fixed(kdir, "q7", 8)
     if "f32" in which:
         make_f32(kdir)
+    if "real" in which:
+        make_real(kdir)
 
 
 if __name__ == "__main__":

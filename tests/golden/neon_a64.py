@@ -9,7 +9,7 @@ time reads the reference.
 Semantics implemented (Arm A64 definitions):
   scalar  ldr/str (B/H/S/D/Q and X registers), ldp/stp, add/sub (immediate,
           register, shifted register), lsl, asr, mul, movz, mov, cmp,
-          b / b.lt / b.ge, ret, adrp + page offsets of read-only data
+          movn, b / b.lt / b.ge, ret, adrp + page offsets of read-only data
   loads   ld1r (replicate one element to every lane), dup (by element)
   FP32    fadd, fsub, fmul (vector and by element), fmla / fmls (vector and
           by element; a fused multiply-add rounded once: the product is
@@ -18,7 +18,8 @@ Semantics implemented (Arm A64 definitions):
           error term)
   integer sqadd, sqsub, srshr, sqrdmulh, smull(2), smlal(2), smlsl(2)
           (vector and by element), sqrshrn(2) on 8- and 16-bit lanes
-  permute rev16, rev32, rev64, zip1, trn1, trn2
+  permute rev16, rev32, rev64, zip1, trn1, trn2, uzp1, uzp2, ext
+  sign    fneg (any lane width: the sign bit flipped), sqneg
 """
 import re
 
@@ -145,10 +146,12 @@ class Machine:
     # ---------------------------------------------------------------
     def call(self, name, args):
         self.x = [0] * 31
-        self.sp = self.stack_top
+        self.sp = self.stack_top - 64  # 16-byte aligned; arguments 9.. live at [sp], [sp + 8], ...
         self.v = [np.zeros(16, np.uint8) for _ in range(32)]
-        for i, a in enumerate(args):
+        for i, a in enumerate(args[:8]):
             self.x[i] = int(a) & MASK64
+        for i, a in enumerate(args[8:]):  # AAPCS64: integer arguments past the eighth on the stack
+            self.mem[self.sp + 8 * i:self.sp + 8 * i + 8] = np.array([int(a) & MASK64], np.uint64).view(np.uint8)
         code = self.k.funcs[name]
         pc, steps = 0, 0
         while True:
@@ -286,6 +289,9 @@ class Machine:
         if op == "movz":
             self.setreg(o[0], self.imm(o[1]))
             return None
+        if op == "movn":
+            self.setreg(o[0], ~self.imm(o[1]))
+            return None
         if op == "mov":
             self.setreg(o[0], self.reg(o[1]))
             return None
@@ -384,6 +390,28 @@ class Machine:
             r = np.empty(n, _INT[w])
             r[0::2], r[1::2] = a[off::2], b[off::2]
             self.put(d, r.astype(np.int64))
+        elif op == "fneg":
+            # flip the sign bit of every lane (exact for any bit pattern)
+            n, w = _ARR[self.arr(d)]
+            a = self.vreg(o[1]).view(_INT[w])[:n].astype(np.int64)
+            self.put(d, a ^ (-(1 << (8 * w - 1))))
+        elif op == "sqneg":
+            _, w = _ARR[self.arr(d)]
+            self.put(d, np.clip(-self.lanes(o[1]), -(1 << (8 * w - 1)), (1 << (8 * w - 1)) - 1))
+        elif op in ("uzp1", "uzp2"):
+            n, w = _ARR[self.arr(d)]
+            a = self.vreg(o[1]).view(_INT[w])[:n].copy()
+            b = self.vreg(o[2]).view(_INT[w])[:n].copy()
+            off = 0 if op == "uzp1" else 1
+            self.put(d, np.concatenate([a[off::2], b[off::2]]).astype(np.int64))
+        elif op == "ext":
+            n, _ = _ARR[self.arr(d)]
+            cat = np.concatenate([self.vreg(o[1])[:n].copy(), self.vreg(o[2])[:n].copy()])
+            i = self.imm(o[3])
+            v = self.vreg(d)
+            v[:n] = cat[i:i + n]
+            if n == 8:
+                v[8:] = 0
         elif op == "dup":
             n, w = _ARR[self.arr(d)]
             self.put(d, np.full(n, self.elem(o[1]), np.int64))

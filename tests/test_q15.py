@@ -3,7 +3,7 @@
 tests/golden/q15_reference.npz holds outputs of the reference's own NEON
 Q0.15 kernels (src/providers/aot/asm/neon/plfft_*q15*.S), executed from
 their source text by tests/golden/neon_a64.py and composed as the
-reference's ESTIMATE plan by tests/golden/ref_c2c_plan.py
+reference's ESTIMATE plan by tests/golden/ref_plan.py
 (tests/golden/make_ref_golden.py).  The C
 restatement oracle/q15.c must reproduce them bit for bit.  It must also
 meet the reference's own fixed-point accuracy bound: 6 * log2(n) LSB

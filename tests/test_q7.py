@@ -4,7 +4,7 @@ tests/golden/q7_reference.npz holds outputs of the reference's own NEON
 Q0.7 kernels (src/providers/aot/asm/neon/plfft_q7_pppn_*.S,
 plfft_ab_q7_pppt_dit_*.S, plfft_ac_q7_pppt_dit_uu.S) executed from their
 source text by tests/golden/neon_a64.py and composed as the reference's
-ESTIMATE plans (tests/golden/ref_c2c_plan.py).  The C restatement
+ESTIMATE plans (tests/golden/ref_plan.py).  The C restatement
 oracle/fixed.c must reproduce them bit for bit for every power-of-two N up
 to 4096, both directions, including saturating inputs.  It must also meet
 the reference's own fixed-point accuracy bound: 6 * log2(n) LSB against the
