@@ -4,8 +4,10 @@
 // decompositions within a budget and keep the fastest, remembering the
 // choice per problem (src/plfft.cpp:149-184, src/planner/benchmarker.hpp:
 // 33-93, src/planner/wisdom.hpp:23-37).  Here the candidates are device
-// schedules for the same C2C problem (make_c2c_candidates): launch shapes,
-// kernel families, four-step shapes.  Each is run on scratch device buffers
+// schedules for the same problem: for C2C (make_c2c_candidates) launch
+// shapes, kernel families, four-step shapes; for R2C, C2R and the R2R kinds
+// (make_real_candidates) the fused kernel's launch shapes and the real-wrap
+// schedule.  Each is run on scratch device buffers
 // with the plan's layout and timed with CUDA events: one warm-up, then
 // rounds of k executions (k calibrated so a round lasts >= 50 us), 3 to 7
 // rounds, median per execution.  The default schedule is timed first and a
@@ -125,18 +127,21 @@ double time_node(const Node& node, const void* in, void* out, void* ws, cudaStre
 }  // namespace
 
 std::string wisdom_key(const ConfigData& c) {
+  static const char* kinds[] = {"c2c", "r2c", "c2r", "r2r"};
   std::ostringstream o;
-  o << "c2c n=" << c.n << " hm=" << c.howmany << " is=" << c.istride << " id=" << c.idist << " os=" << c.ostride
-    << " od=" << c.odist << " dir=" << c.payload << " scaled=" << (c.scale != 1.0) << " prec=" << c.precision
-    << " dev=" << device_name();
+  o << kinds[int(c.kind)] << " n=" << c.n << " hm=" << c.howmany << " is=" << c.istride << " id=" << c.idist
+    << " os=" << c.ostride << " od=" << c.odist << " dir=" << c.payload << " scaled=" << (c.scale != 1.0)
+    << " prec=" << c.precision << " dev=" << device_name();
   return o.str();
 }
 
-std::unique_ptr<Node> autotune_c2c(const ConfigData& c, const Layout& lay, std::string* why, std::string* note) {
-  const int level = c.rigor == PLFFT_MEASURE ? 1 : (c.rigor == PLFFT_PATIENT ? 2 : 3);
+namespace {
+
+// Times the candidates (default first) on scratch buffers of the plan's
+// spans and keeps the fastest; the wisdom key remembers the choice.
+std::unique_ptr<Node> tune(const ConfigData& c, std::vector<std::unique_ptr<Node>> cands, int64_t nin, int64_t nout,
+                           size_t in_elem, size_t out_elem, std::string* note) {
   const double budget = c.rigor == PLFFT_MEASURE ? 0.1 : (c.rigor == PLFFT_PATIENT ? 0.5 : 2.0);
-  auto cands = make_c2c_candidates(c.n, lay, c.payload, float(c.scale), c.precision, level);
-  if (cands.empty()) return make_c2c_node(c.n, lay, c.payload, float(c.scale), c.precision, why);
   const std::string key = wisdom_key(c);
   std::string known;
   if (recall(key, known)) {
@@ -151,8 +156,8 @@ std::unique_ptr<Node> autotune_c2c(const ConfigData& c, const Layout& lay, std::
   size_t ws_bytes = 0;
   for (auto& cand : cands) ws_bytes = std::max(ws_bytes, cand->workspace());
   DevBuf din, dout, dws;
-  const size_t ib = size_t(span(c.howmany, c.idist, c.n, c.istride)) * sizeof(float2);
-  const size_t ob = size_t(span(c.howmany, c.odist, c.n, c.ostride)) * sizeof(float2);
+  const size_t ib = size_t(span(c.howmany, c.idist, nin, c.istride)) * in_elem;
+  const size_t ob = size_t(span(c.howmany, c.odist, nout, c.ostride)) * out_elem;
   cudaStream_t st = nullptr;
   if (din.alloc(ib) != cudaSuccess || dout.alloc(ob) != cudaSuccess || dws.alloc(ws_bytes) != cudaSuccess ||
       cudaMemset(din.p, 0, ib) != cudaSuccess || cudaStreamCreate(&st) != cudaSuccess) {
@@ -184,6 +189,26 @@ std::unique_ptr<Node> autotune_c2c(const ConfigData& c, const Layout& lay, std::
   }
   remember(key, cands[best]->describe());
   return std::move(cands[best]);
+}
+
+int tune_level(const ConfigData& c) { return c.rigor == PLFFT_MEASURE ? 1 : (c.rigor == PLFFT_PATIENT ? 2 : 3); }
+
+}  // namespace
+
+std::unique_ptr<Node> autotune_c2c(const ConfigData& c, const Layout& lay, std::string* why, std::string* note) {
+  auto cands = make_c2c_candidates(c.n, lay, c.payload, float(c.scale), c.precision, tune_level(c));
+  if (cands.empty()) return make_c2c_node(c.n, lay, c.payload, float(c.scale), c.precision, why);
+  return tune(c, std::move(cands), c.n, c.n, sizeof(float2), sizeof(float2), note);
+}
+
+std::unique_ptr<Node> autotune_real(const ConfigData& c, const Layout& lay, int fused_kind, int wrap_kind,
+                                    std::string* why, std::string* note) {
+  auto cands = make_real_candidates(fused_kind, wrap_kind, c.n, lay, float(c.scale), tune_level(c));
+  if (cands.empty()) return make_realwrap_node(wrap_kind, c.n, lay, c.scale, why);
+  const int64_t h = c.n / 2 + 1;
+  const bool cin = c.kind == TKind::C2R, cout = c.kind == TKind::R2C;
+  return tune(c, std::move(cands), cin ? h : c.n, cout ? h : c.n, cin ? sizeof(float2) : sizeof(float),
+              cout ? sizeof(float2) : sizeof(float), note);
 }
 
 }  // namespace plfft_b200

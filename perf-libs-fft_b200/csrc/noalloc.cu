@@ -24,8 +24,17 @@
 // carries over from the previous call.  Calls whose execution overlaps on the
 // GPU (different streams without ordering between them) race on the array
 // and must not be issued.
+//
+// Cost per call: one table-fill launch, then two launches per chunk of
+// members (a chunk is as many members as fit the 16 MiB buffer), all on the
+// caller's stream.  After the first call on a device the cached address is
+// read without taking a lock.  The cache lives as long as the process's
+// context on that device: after cudaDeviceReset the next call must not be
+// made through this entry point until the process restarts, since the array
+// is re-created at a new address.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <mutex>
 
 #include "../../include/plfft.h"
@@ -46,20 +55,23 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 constexpr int kNoAllocMaxDevices = 64;
 static std::mutex g_noalloc_mu;
-static void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+static std::atomic<void*> g_noalloc_addr[kNoAllocMaxDevices] = {};
 
 // device address of g_noalloc_scratch on the current device (looked up once
-// per device)
+// per device, under a lock; later calls read it without one)
 static cudaError_t noalloc_scratch(int dev, unsigned char** out) {
   if (dev < 0 || dev >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    g_noalloc_addr[dev] = p;
+  void* p = g_noalloc_addr[dev].load(std::memory_order_acquire);
+  if (!p) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    p = g_noalloc_addr[dev].load(std::memory_order_relaxed);
+    if (!p) {
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess) return e;
+      g_noalloc_addr[dev].store(p, std::memory_order_release);
+    }
   }
-  *out = static_cast<unsigned char*>(g_noalloc_addr[dev]);
+  *out = static_cast<unsigned char*>(p);
   return cudaSuccess;
 }
 

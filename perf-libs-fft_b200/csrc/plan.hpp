@@ -199,7 +199,18 @@ std::unique_ptr<Node> make_fp64_c2c(int64_t n, const Layout& lay, int dir, doubl
 // One-kernel R2C / C2R / DCT-II / DST-II (FusedRealKind) for N = 2M, M a
 // power of two in [64, 8192], unit strides; nullptr when not applicable.
 // wmode: adjoint weights (RealFusedLaunch::wmode), 0 for the plain transform.
-std::unique_ptr<Node> make_real_fused_node(int kind, int64_t n, const Layout& lay, float scale, int wmode = 0);
+std::unique_ptr<Node> make_real_fused_node(int kind, int64_t n, const Layout& lay, float scale, int wmode = 0,
+                                           int g_override = 0, int e_override = 0);
+
+// Alternative schedules of a real-data transform (fused kind or -1, the
+// real-wrap kind), the default first, for the autotuner.
+std::vector<std::unique_ptr<Node>> make_real_candidates(int fused_kind, int wrap_kind, int64_t n, const Layout& lay,
+                                                        float scale, int level);
+
+// Plan-time autotuning of a real-data transform (rigor above ESTIMATE):
+// times make_real_candidates and remembers the winner in wisdom.
+std::unique_ptr<Node> autotune_real(const ConfigData& c, const Layout& lay, int fused_kind, int wrap_kind,
+                                    std::string* why, std::string* note);
 
 // Adjoint of a plan's transform (same scale, input/output layouts swapped):
 // the conjugate-direction C2C, or the transposed real transform expressed

@@ -59,14 +59,28 @@ static std::unique_ptr<Node> make_root(const ConfigData& c, const Layout& lay, b
           root = autotune_c2c(c, lay, why, note);
         break;
       case TKind::R2C:
+        if (tune && c.rigor != PLFFT_ESTIMATE) {
+          root = autotune_real(c, lay, FR_R2C, RW_R2C, why, note);
+          break;
+        }
         root = make_real_fused_node(FR_R2C, c.n, lay, scale);
         if (!root) root = make_realwrap_node(RW_R2C, c.n, lay, scale, why);
         break;
       case TKind::C2R:
+        if (tune && c.rigor != PLFFT_ESTIMATE) {
+          root = autotune_real(c, lay, FR_C2R, RW_C2R, why, note);
+          break;
+        }
         root = make_real_fused_node(FR_C2R, c.n, lay, scale);
         if (!root) root = make_realwrap_node(RW_C2R, c.n, lay, scale, why);
         break;
       case TKind::R2R: {
+        if (tune && c.rigor != PLFFT_ESTIMATE) {
+          static const int fused_of[] = {-1, FR_DCT2, FR_DCT3, FR_DCT4, -1, FR_DST2,
+                                         FR_DST3, FR_DST4, FR_DHT, FR_R2HC, FR_HC2R};
+          root = autotune_real(c, lay, fused_of[c.payload], r2r_wrap_kind(c.payload), why, note);
+          break;
+        }
         if (c.payload == PLFFT_R2R_DCT_2) root = make_real_fused_node(FR_DCT2, c.n, lay, scale);
         if (c.payload == PLFFT_R2R_DST_2) root = make_real_fused_node(FR_DST2, c.n, lay, scale);
         if (c.payload == PLFFT_R2R_DCT_3) root = make_real_fused_node(FR_DCT3, c.n, lay, scale);

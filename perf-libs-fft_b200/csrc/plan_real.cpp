@@ -147,13 +147,15 @@ struct RealFusedNode : Node {
 
 }  // namespace
 
-std::unique_ptr<Node> make_real_fused_node(int kind, int64_t n, const Layout& lay, float scale, int wmode) {
+std::unique_ptr<Node> make_real_fused_node(int kind, int64_t n, const Layout& lay, float scale, int wmode, int g_override,
+                                           int e_override) {
   if (n % 2 || !real_fused_supported(int(n / 2)) || lay.istride != 1 || lay.ostride != 1) return nullptr;
   if (std::getenv("PLFFT_B200_NO_FUSED_REAL")) return nullptr;
   const int m = int(n / 2);
   int e = real_fused_e(m);
   if (const char* v = std::getenv("PLFFT_B200_RF_E"))  // launch-shape experiments
     if (m == 512 && std::atoi(v) == 32) e = 32;
+  if (e_override && (e_override == e || (m == 512 && e_override == 32))) e = e_override;
   std::vector<int> radices;
   int rest = m, ke = 0;
   while (rest % e == 0 && rest > 1) {
@@ -187,6 +189,8 @@ std::unique_ptr<Node> make_real_fused_node(int kind, int64_t n, const Layout& la
   node->base.odist = lay.odist;
   node->base.g = std::max(1, 128 / t);
   if (const char* v = std::getenv("PLFFT_B200_RF_G")) node->base.g = std::max(1, std::atoi(v));
+  if (g_override) node->base.g = g_override;
+  if (t * node->base.g > 1024) return nullptr;
   node->base.g = std::max(node->base.g, std::max(1, 32 / t));  // whole warps (the kernel shuffles)
   node->base.e = e;
   node->base.wmode = wmode;
@@ -195,6 +199,46 @@ std::unique_ptr<Node> make_real_fused_node(int kind, int64_t n, const Layout& la
   node->base.post = node->tab.as<float2>() + post_off;
   node->base.rot = node->tab.as<float2>() + rot_off;
   return node;
+}
+
+}  // namespace plfft_b200
+
+namespace plfft_b200 {
+
+// Alternative schedules of a real-data transform for the autotuner, the
+// default first: the fused kernel with other transforms-per-CTA counts and
+// (N = 1024) the other register split, then the three-launch real-wrap
+// schedule around a C2C.
+std::vector<std::unique_ptr<Node>> make_real_candidates(int fused_kind, int wrap_kind, int64_t n, const Layout& lay,
+                                                        float scale, int level) {
+  std::vector<std::unique_ptr<Node>> out;
+  std::string why;
+  auto fused = fused_kind >= 0 ? make_real_fused_node(fused_kind, n, lay, scale) : nullptr;
+  if (fused) {
+    const int g0 = static_cast<RealFusedNode*>(fused.get())->base.g;
+    const int e0 = static_cast<RealFusedNode*>(fused.get())->base.e;
+    out.push_back(std::move(fused));
+    for (int g : {g0 / 2, g0 * 2, g0 / 4, g0 * 4}) {
+      if (g < 1 || g == g0) continue;
+      if (auto c = make_real_fused_node(fused_kind, n, lay, scale, 0, g)) out.push_back(std::move(c));
+    }
+    if (n == 1024) {
+      for (int g : {g0, g0 / 2, g0 * 2})
+        if (g >= 1)
+          if (auto c = make_real_fused_node(fused_kind, n, lay, scale, 0, g, e0 == 16 ? 32 : 16)) out.push_back(std::move(c));
+    }
+  }
+  if (out.empty() || level >= 2) {
+    if (auto w = make_realwrap_node(wrap_kind, n, lay, scale, &why)) out.push_back(std::move(w));
+  }
+  // keep the first of schedules that describe alike
+  std::vector<std::unique_ptr<Node>> uniq;
+  for (auto& c : out) {
+    bool dup = false;
+    for (auto& u : uniq) dup = dup || u->describe() == c->describe();
+    if (!dup) uniq.push_back(std::move(c));
+  }
+  return uniq;
 }
 
 }  // namespace plfft_b200
