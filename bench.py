@@ -879,6 +879,19 @@ def reference_arm(w, steps, warmup, budget_s=120.0):
                    "sample": f"{text}, {reps} repetitions per step"}, dt * 1e3 / steps
 
 
+def max_over_ranks(dist, values, device):
+    """Element-wise maximum over ranks of per-rank figures (step counts,
+    device-timed milliseconds).  Every rank makes the same collective call
+    in the same order; without a process group the values pass through."""
+    import torch
+
+    if dist is None:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 # --------------------------------------------------------------------------
 def parse():
     ap = argparse.ArgumentParser()
@@ -953,12 +966,9 @@ def main():
         ev1.record(stream)
         torch.cuda.synchronize()
         est = ev0.elapsed_time(ev1) / 20
-        steps = [max(200, min(200000, int(1000.0 / max(est, 1e-4))))]
-        if dist is not None:  # every rank times the same number of steps
-            t = torch.tensor(steps, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            steps = [int(t.item())]
-        args.steps = steps[0]
+        steps = max(200, min(200000, int(1000.0 / max(est, 1e-4))))
+        # every rank times the same number of steps
+        args.steps = int(max_over_ranks(dist, [steps], "cuda")[0])
     barrier()
     torch.cuda.synchronize()
     sampler.mark()
@@ -990,9 +1000,7 @@ def main():
                "h2d_bytes_per_step": hb, "d2h_bytes_per_step": db, "ms_per_step": e2e_ms, "api": api}
 
     if dist is not None:
-        t = torch.tensor([ms, step_ms, e2e["ms_per_step"] if e2e else 0.0], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, step_ms, e2e_max = [float(v) for v in t.tolist()]
+        ms, step_ms, e2e_max = max_over_ranks(dist, [ms, step_ms, e2e["ms_per_step"] if e2e else 0.0], "cuda")
         if e2e:
             e2e["ms_per_step"] = e2e_max
             e2e["value"] = w.algo_bytes() * world / (e2e_max * 1e-3) / 1e9

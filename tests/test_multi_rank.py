@@ -71,3 +71,43 @@ def test_two_rank_batch_shards_match_whole_batch():
         p.join(120)
         assert p.exitcode == 0
     assert q.get(timeout=5) == 0.0
+
+
+def _bench_worker(rank, world, port, q):
+    import torch.distributed as dist
+
+    import bench
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    # each rank's own step count and timings; the bench line must use the maximum
+    steps = bench.max_over_ranks(dist, [200 + 50 * rank], "cpu")
+    ms = bench.max_over_ranks(dist, [1.5 - rank, 0.25 * (rank + 1), 0.0], "cpu")
+    q.put((rank, steps, ms))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_bench_max_over_ranks_two_gloo_ranks():
+    """bench.py's multi-rank reduction (one process per GPU under torchrun):
+    every rank times the same step count and reports the slowest rank's time."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 31500 + os.getpid() % 2000
+    procs = [ctx.Process(target=_bench_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    got = sorted(q.get(timeout=5) for _ in range(2))
+    for _, steps, ms in got:
+        assert steps == [250.0]
+        assert ms == [1.5, 0.5, 0.0]
+
+
+def test_bench_max_over_ranks_single_process():
+    import bench
+
+    assert bench.max_over_ranks(None, [3, 1.5], "cpu") == [3.0, 1.5]
