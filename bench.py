@@ -708,7 +708,7 @@ def make_workload(name):
         # kernel-coverage workloads (not benchmark configurations): the
         # smooth non-power-of-two, Rader, Bluestein and real-wrap schedules
         "c2c_n1000_b16384": lambda: PlanWorkload("c2c_n1000_b16384", "C2C FP32 N=1000 (2^3 5^3) batch=16384",
-                                                 "c2c", 1000, 16384, profile="c2c_reg_n1000_b16384"),
+                                                 "c2c", 1000, 16384, profile="c2c_tile_n1000_b16384"),
         "c2c_n1009_b8192": lambda: PlanWorkload("c2c_n1009_b8192", "C2C FP32 N=1009 (Rader) batch=8192",
                                                 "c2c", 1009, 8192, profile="conv_rader_n1009_b8192"),
         "c2c_n1031_b8192": lambda: PlanWorkload("c2c_n1031_b8192", "C2C FP32 N=1031 (Bluestein) batch=8192",
