@@ -711,8 +711,8 @@ def make_workload(name):
                                                  "c2c", 1000, 16384, profile="c2c_tile_n1000_b16384"),
         "c2c_n1009_b8192": lambda: PlanWorkload("c2c_n1009_b8192", "C2C FP32 N=1009 (Rader) batch=8192",
                                                 "c2c", 1009, 8192, profile="conv_rader_n1009_b8192"),
-        "c2c_n1031_b8192": lambda: PlanWorkload("c2c_n1031_b8192", "C2C FP32 N=1031 (Bluestein) batch=8192",
-                                                "c2c", 1031, 8192, profile="conv_bluestein_n1031_b8192"),
+        "c2c_n1034_b8192": lambda: PlanWorkload("c2c_n1034_b8192", "C2C FP32 N=1034 (2 11 47, Bluestein) batch=8192",
+                                                "c2c", 1034, 8192, profile="conv_bluestein_n1034_b8192"),
         "r2c_n1000_b16384": lambda: PlanWorkload("r2c_n1000_b16384", "R2C FP32 N=1000 (real wrap) batch=16384",
                                                  "r2c", 1000, 16384, profile="realwrap_r2c_n1000_b16384"),
     }
@@ -723,7 +723,7 @@ WORKLOAD_NAMES = ["c2c_n1024_b4096", "r2c_c2r_n4096_b8192", "dct2_n1024_b4096", 
                   "c2c_n64k_b1024", "c2c_n1m_b64_split_bf16", "c2c_n64k_b1024_split_bf16", "grouped_4000",
                   "grouped_4000_per_length",
                   "diff_r2c_n8192_b1024", "q15_n256_b16384",
-                  "c2c_n1000_b16384", "c2c_n1009_b8192", "c2c_n1031_b8192", "r2c_n1000_b16384"]
+                  "c2c_n1000_b16384", "c2c_n1009_b8192", "c2c_n1034_b8192", "r2c_n1000_b16384"]
 
 
 # --------------------------------------------------------------------------

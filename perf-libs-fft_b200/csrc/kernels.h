@@ -4,6 +4,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+#include <vector>
+
 #include "stockham_desc.h"
 
 namespace plfft_b200 {
@@ -146,6 +149,30 @@ struct ConvLaunch {
   float scale;
 };
 cudaError_t launch_conv(int step, const ConvLaunch& L, int64_t m0, int64_t cnt, cudaStream_t st);
+
+// One-kernel Rader / Bluestein over power-of-two convolution lengths
+// 64 <= m <= 8192 (conv_fused.cu)
+struct ConvFusedLaunch {
+  const float2* in;
+  float2* out;
+  int64_t howmany, istride, idist, ostride, odist;
+  int n;                // transform length (the prime P for Rader)
+  int g;                // members per CTA
+  const float2* tw;     // stage twiddles of the length-m power-of-two stage list
+  const float2* chirp;  // Bluestein w_k, k < n
+  const float2* spec;   // FFT_m(b) / m
+  const int* perm_in;   // Rader g^q mod P, q < P - 1
+  const int* perm_out;  // Rader g^-q mod P
+  float scale;
+};
+// Shape of a launch: e elements per thread (16 or 32) and minb, the resident
+// 256-thread CTAs per SM the register allocation is sized for (2, 3, 4:
+// 128, 85, 64 registers per thread).  conv_fused_shapes(m) lists the
+// instantiated shapes for m, the default first.
+std::vector<std::pair<int, int>> conv_fused_shapes(int m);
+bool conv_fused_supported(int m, int e, int minb);
+int conv_fused_smem_bytes(int m, int g);
+cudaError_t launch_conv_fused(int m, int e, int minb, bool rader, const ConvFusedLaunch& L, cudaStream_t st);
 
 // Grouped mixed-length execution (grouped.cu)
 enum GTaskType { GT_TILE = 0, GT_RADER = 1, GT_BLUE = 2 };

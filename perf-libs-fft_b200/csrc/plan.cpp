@@ -814,6 +814,18 @@ std::vector<std::unique_ptr<Node>> make_c2c_candidates(int64_t n, const Layout& 
     Addr oa{lay.odist, 0, lay.ostride, 1};
     if (auto t = make_tile(n, lay.howmany, ia, oa, dir, scale, interleaved, &why)) out.push_back(std::move(t));
   }
+  if (!is_smooth(n) && conv_fused_length(n)) {
+    // shapes of the one-launch convolution kernel, and members per CTA
+    const int64_t m = conv_fused_length(n);
+    for (const auto& sh : conv_fused_shapes(int(m))) {
+      const int t = int(m / sh.first);
+      const int gdef = std::max(1, 64 / t);
+      for (int g : {gdef, 2 * gdef, gdef / 2}) {
+        if (g < 1 || g * t > std::max(256, t) || (g != gdef && level < 2)) continue;
+        if (auto c = make_conv_fused(n, lay, dir, scale, &why, sh.first, sh.second, g)) out.push_back(std::move(c));
+      }
+    }
+  }
   if (is_pow2(n) && n > 8192) {
     // the one-pass cluster form (one HBM round trip, but latency-bound at
     // 8 warps per SM: 1.13 TB/s against 1.8 for two passes at 2^16 x 1024)

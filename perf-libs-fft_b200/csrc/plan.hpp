@@ -185,6 +185,11 @@ int64_t primitive_root(int64_t p);
 
 // Rader (prime n, smooth n-1) or Bluestein (any n) convolution node.
 std::unique_ptr<Node> make_conv_node(int64_t n, const Layout& lay, int dir, float scale, std::string* why);
+// one-launch Rader / Bluestein when the convolution fits a power-of-two
+// length <= 8192 (conv_fused_length(n) != 0); e = 0 picks the default shape
+int64_t conv_fused_length(int64_t n);
+std::unique_ptr<Node> make_conv_fused(int64_t n, const Layout& lay, int dir, float scale, std::string* why, int e,
+                                      int minb, int g);
 int64_t next_smooth(int64_t n);
 
 // R2C / C2R / R2R through a C2C plan of a related length (realwrap.cu);

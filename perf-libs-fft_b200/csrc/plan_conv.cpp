@@ -168,7 +168,196 @@ struct ConvNode : Node {
 
 }  // namespace
 
+// Convolution tables.  Bluestein: w_k = exp(dir i pi (k^2 mod 2n) / n).
+static std::vector<cd> bluestein_chirp(int64_t n, int dir) {
+  std::vector<cd> w(n);
+  for (int64_t k = 0; k < n; ++k) {
+    const int64_t e = int64_t((__int128)k * k % (2 * n));
+    double c, s;
+    unit_root(e, 2 * n, c, s);
+    w[k] = cd(c, dir * s);
+  }
+  return w;
+}
+
+// b_m = conj(w_|m|) for |m| < n, placed cyclically in a length-m sequence
+// (m >= 2n - 1)
+static std::vector<cd> bluestein_kernel(const std::vector<cd>& w, int64_t m) {
+  const int64_t n = int64_t(w.size());
+  std::vector<cd> b(m, cd(0, 0));
+  for (int64_t k = 0; k < n; ++k) {
+    b[k] = std::conj(w[k]);
+    if (k) b[m - k] = std::conj(w[k]);
+  }
+  return b;
+}
+
+// Rader for prime p with generator g, l = p - 1: perm_in[q] = g^q,
+// perm_out[q] = g^-q, and b_q = exp(dir 2 pi i g^-q / p) laid out for a
+// length-m cyclic convolution (m = l exactly, or m >= 2l - 1 with the
+// negative lags b_{l-j} at m - j so a zero-padded input convolves cyclically
+// modulo l)
+static void rader_tables(int64_t p, int dir, int64_t m, std::vector<int>& pin, std::vector<int>& pout,
+                         std::vector<cd>& b) {
+  const int64_t l = p - 1;
+  const int64_t g = primitive_root(p);
+  const int64_t ginv = pow_mod(g, p - 2, p);
+  pin.assign(size_t(l), 0);
+  pout.assign(size_t(l), 0);
+  std::vector<cd> bl(l);
+  int64_t gq = 1, gi = 1;
+  for (int64_t q = 0; q < l; ++q) {
+    pin[q] = int(gq);
+    pout[q] = int(gi);
+    double c, s;
+    unit_root(gi, p, c, s);
+    bl[q] = cd(c, dir * s);
+    gq = gq * g % p;
+    gi = gi * ginv % p;
+  }
+  b.assign(size_t(m), cd(0, 0));
+  for (int64_t j = 0; j < l; ++j) b[j] = bl[j];
+  for (int64_t j = 1; j < l; ++j) b[m - j] = bl[l - j];
+}
+
+namespace {
+
+// One launch per execution: conv_fused_kernel over power-of-two m.
+struct ConvFusedNode : Node {
+  bool rader = false;
+  int64_t n = 0, m = 0;
+  Layout lay{};
+  float scale = 1.f;
+  int e = 16, minb = 3, g = 1;
+  DevBuf tw, chirp, spec, pin, pout;
+  cudaError_t run(const void* in, void* out, void*, cudaStream_t st) const override {
+    ConvFusedLaunch L{};
+    L.in = static_cast<const float2*>(in);
+    L.out = static_cast<float2*>(out);
+    L.howmany = lay.howmany;
+    L.istride = lay.istride;
+    L.idist = lay.idist;
+    L.ostride = lay.ostride;
+    L.odist = lay.odist;
+    L.n = int(n);
+    L.g = g;
+    L.tw = tw.as<float2>();
+    L.chirp = chirp.as<float2>();
+    L.spec = spec.as<float2>();
+    L.perm_in = pin.as<int>();
+    L.perm_out = pout.as<int>();
+    L.scale = scale;
+    return launch_conv_fused(int(m), e, minb, rader, L, st);
+  }
+  std::string describe() const override {
+    std::ostringstream o;
+    o << "(" << (rader ? "rader" : "bluestein") << "-fused n=" << n << " m=" << m << " e=" << e << " minb=" << minb
+      << " g=" << g << ")";
+    return o.str();
+  }
+};
+
+int64_t next_pow2(int64_t v) {
+  int64_t p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+}  // namespace
+
+int64_t conv_fused_length(int64_t n) {
+  if (n < 3) return 0;
+  // Rader convolves l = n - 1 terms, Bluestein n: a cyclic length >= 2l - 1
+  const int64_t m = next_pow2(std::max<int64_t>(64, is_prime(n) ? 2 * n - 3 : 2 * n - 1));
+  return m <= 8192 ? m : 0;
+}
+
+// e = 0: the default shape for the length (PLFFT_B200_CONV_E / _MINB / _G
+// override it), else the given shape
+std::unique_ptr<Node> make_conv_fused(int64_t n, const Layout& lay, int dir, float scale, std::string* why, int e_req,
+                                      int minb_req, int g_req) {
+  if (std::getenv("PLFFT_B200_CONV_UNFUSED")) return nullptr;
+  const int64_t m = conv_fused_length(n);
+  if (m == 0) return nullptr;
+  const bool rader = is_prime(n);
+  const auto shapes = conv_fused_shapes(int(m));
+  if (shapes.empty()) return nullptr;
+  int e = shapes[0].first, minb = shapes[0].second;
+  if (e_req) {
+    e = e_req;
+    minb = minb_req;
+  } else {
+    if (const char* v = std::getenv("PLFFT_B200_CONV_E")) e = std::atoi(v);
+    if (const char* v = std::getenv("PLFFT_B200_CONV_MINB")) minb = std::atoi(v);
+    if (!conv_fused_supported(int(m), e, minb))
+      for (const auto& sh : shapes)
+        if (sh.first == e) {
+          minb = sh.second;
+          break;
+        }
+  }
+  if (!conv_fused_supported(int(m), e, minb)) {
+    if (e_req) return nullptr;
+    e = shapes[0].first;
+    minb = shapes[0].second;
+  }
+  auto node = std::make_unique<ConvFusedNode>();
+  node->rader = rader;
+  node->n = n;
+  node->m = m;
+  node->lay = lay;
+  node->scale = scale;
+  node->e = e;
+  node->minb = minb;
+  const int t = int(m / e);
+  const int maxthr = t > 256 ? t : 256;
+  int g = std::max(1, 64 / t);
+  if (g_req > 0)
+    g = g_req;
+  else if (const char* v = std::getenv("PLFFT_B200_CONV_G"))
+    g = std::max(1, std::atoi(v));
+  while (g > 1 && (g * t > maxthr || conv_fused_smem_bytes(int(m), g) > 160 * 1024)) g /= 2;
+  node->g = g;
+  // radices: leftover factor first, then radix-e stages (the order of the
+  // compile-time stage list)
+  std::vector<int> radices;
+  int64_t rest = m;
+  int ke = 0;
+  while (rest % e == 0 && rest > 1) {
+    rest /= e;
+    ++ke;
+  }
+  if (rest > 1) radices.push_back(int(rest));
+  for (int i = 0; i < ke; ++i) radices.push_back(e);
+  std::vector<float2> tw;
+  make_desc(int(m), radices, tw);
+  std::vector<cd> b;
+  cudaError_t err = node->tw.upload(tw);
+  if (rader) {
+    std::vector<int> pin, pout;
+    rader_tables(n, dir, m, pin, pout, b);
+    if (err == cudaSuccess) err = node->pin.upload(pin);
+    if (err == cudaSuccess) err = node->pout.upload(pout);
+  } else {
+    const std::vector<cd> w = bluestein_chirp(n, dir);
+    b = bluestein_kernel(w, m);
+    if (err == cudaSuccess) err = node->chirp.upload(to_f2(w, 1.0));
+  }
+  if (err == cudaSuccess) err = node->spec.upload(to_f2(host_fft(b, -1), 1.0 / double(m)));
+  if (err != cudaSuccess) {
+    if (why) *why = "device allocation failed";
+    return nullptr;
+  }
+  return node;
+}
+
+// Strategy: lengths whose convolution fits a power-of-two m <= 8192 run as
+// one fused launch (Rader for every prime, since its m never exceeds
+// Bluestein's); longer ones follow the reference planner's rule (Rader for
+// prime n with smooth n - 1, else Bluestein over the smallest smooth
+// m >= 2n - 1) with multi-launch length-m C2C plans.
 std::unique_ptr<Node> make_conv_node(int64_t n, const Layout& lay, int dir, float scale, std::string* why) {
+  if (auto f = make_conv_fused(n, lay, dir, scale, why, 0, 0, 0)) return f;
   auto node = std::make_unique<ConvNode>();
   node->dir = dir;
   node->n = n;
@@ -184,45 +373,20 @@ std::unique_ptr<Node> make_conv_node(int64_t n, const Layout& lay, int dir, floa
   node->bwd = make_c2c_node(m, inner, +1, 1.0f, 0, why);
   if (!node->fwd || !node->bwd) return nullptr;
 
-  std::vector<cd> b(m, cd(0, 0));
+  std::vector<cd> b;
+  cudaError_t err = cudaSuccess;
   if (node->rader) {
-    const int64_t g = primitive_root(n);
-    const int64_t ginv = pow_mod(g, n - 2, n);
-    std::vector<int> pin(m), pout(m);
-    int64_t gq = 1, gi = 1;
-    for (int64_t q = 0; q < m; ++q) {
-      pin[q] = int(gq);
-      pout[q] = int(gi);
-      double c, s;
-      unit_root(gi, n, c, s);  // b_q = exp(dir 2 pi i g^-q / P)
-      b[q] = cd(c, dir * s);
-      gq = gq * g % n;
-      gi = gi * ginv % n;
-    }
-    if (node->pin.upload(pin) != cudaSuccess || node->pout.upload(pout) != cudaSuccess) {
-      if (why) *why = "device allocation failed";
-      return nullptr;
-    }
+    std::vector<int> pin, pout;
+    rader_tables(n, dir, m, pin, pout, b);
+    err = node->pin.upload(pin);
+    if (err == cudaSuccess) err = node->pout.upload(pout);
   } else {
-    // w_k = exp(dir i pi (k^2 mod 2n) / n); b_m = conj(w_m), wrapped
-    std::vector<cd> w(n);
-    for (int64_t k = 0; k < n; ++k) {
-      const int64_t e = int64_t((__int128)k * k % (2 * n));
-      double c, s;
-      unit_root(e, 2 * n, c, s);
-      w[k] = cd(c, dir * s);
-    }
-    for (int64_t k = 0; k < n; ++k) {
-      b[k] = std::conj(w[k]);
-      if (k) b[m - k] = std::conj(w[k]);
-    }
-    if (node->chirp.upload(to_f2(w, 1.0)) != cudaSuccess) {
-      if (why) *why = "device allocation failed";
-      return nullptr;
-    }
+    const std::vector<cd> w = bluestein_chirp(n, dir);
+    b = bluestein_kernel(w, m);
+    err = node->chirp.upload(to_f2(w, 1.0));
   }
-  const std::vector<cd> B = host_fft(b, -1);
-  if (node->spec.upload(to_f2(B, 1.0 / double(m))) != cudaSuccess) {
+  if (err == cudaSuccess) err = node->spec.upload(to_f2(host_fft(b, -1), 1.0 / double(m)));
+  if (err != cudaSuccess) {
     if (why) *why = "device allocation failed";
     return nullptr;
   }

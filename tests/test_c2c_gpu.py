@@ -52,14 +52,41 @@ def test_c2c_reference_conv_layouts(case, direction):
     assert oracle.rel_l2(got, ref) <= oracle.fp32_tol(n), plan.describe()
 
 
-@pytest.mark.parametrize("n", [17, 23, 97, 1009, 4099, 1031, 1058, 2870, 2 * 8191, 65537, 8191 * 3])
+# (n, schedule): one fused launch while the convolution fits a power-of-two
+# m <= 8192 (Rader for every prime p <= 4097: m >= 2p - 3; Bluestein for
+# other lengths n <= 4096: m >= 2n - 1), multi-launch convolutions beyond
+CONV_CASES = [(17, "rader-fused"), (23, "rader-fused"), (47, "rader-fused"), (97, "rader-fused"),
+              (1009, "rader-fused"), (1031, "rader-fused"), (4093, "rader-fused"), (94, "bluestein-fused"),
+              (1034, "bluestein-fused"),
+              (1058, "bluestein-fused"), (2870, "bluestein-fused"), (4094, "bluestein-fused"),
+              (4099, "(bluestein n="), (2 * 8191, "(bluestein n="), (65537, "(rader n="), (8191 * 3, "(bluestein n=")]
+
+
+@pytest.mark.parametrize("n,expect", CONV_CASES)
 @pytest.mark.parametrize("direction", [-1, 1])
-def test_c2c_rader_bluestein(n, direction):
+def test_c2c_rader_bluestein(n, expect, direction):
     howmany = 3
     got, ref, plan = c2c_case(n, howmany, direction=direction, seed=n, method="fft")
-    expect = "rader" if n in (17, 23, 97, 1009, 65537) else "bluestein"
     assert expect in plan.describe(), plan.describe()
     assert oracle.rel_l2(got, ref) <= oracle.fp32_tol(n), plan.describe()
+
+
+# the fused convolution kernel's launch shapes: 16 or 32 elements per thread,
+# each register budget, several members per CTA (the last CTA partly
+# filled), strided members
+@pytest.mark.parametrize("e,minb", [(16, 2), (16, 3), (16, 4), (32, 2)])
+@pytest.mark.parametrize("n,hm,layout", [(17, 37, (1, 17, 1, 17)), (1009, 11, (1, 1009, 1, 1009)),
+                                         (1034, 9, (9, 1, 9, 1)), (4093, 5, (1, 4093, 1, 4093)),
+                                         (300 * 7 - 1, 4, (1, 2099, 1, 2100)), (263, 33, (2, 600, 1, 263))])
+def test_c2c_conv_fused_shapes(monkeypatch, e, minb, n, hm, layout):
+    monkeypatch.setenv("PLFFT_B200_CONV_E", str(e))
+    monkeypatch.setenv("PLFFT_B200_CONV_MINB", str(minb))
+    monkeypatch.setenv("PLFFT_B200_CONV_G", "4")
+    is_, id_, os_, od = layout
+    for direction in (-1, 1):
+        got, ref, plan = c2c_case(n, hm, is_, id_, os_, od, direction=direction, seed=n + e, method="fft")
+        assert "fused" in plan.describe(), plan.describe()
+        assert oracle.rel_l2(got, ref) <= oracle.fp32_tol(n), plan.describe()
 
 
 @pytest.mark.parametrize("n", [32768, 65536, 1 << 18, 1 << 20])

@@ -4,7 +4,8 @@ calling plfft_plan_execute on one plan from several threads at once).
 On the device this is stream-ordered execution on two streams with a
 workspace each (plfft_cuda_execute_async): the two executions may overlap on
 the GPU and must not share scratch.  The schedules used need workspace:
-the two-pass four-step (n = 65536) and a Bluestein convolution (n = 1031).
+the two-pass four-step (n = 65536) and a multi-launch Bluestein convolution
+(n = 4099).
 On the host, two threads call plfft_plan_execute on the same plan with
 their own host buffers.
 """
@@ -28,7 +29,7 @@ def _rand(n, hm, seed):
                          torch.rand(n * hm, device="cuda", generator=g) * 2 - 1)
 
 
-@pytest.mark.parametrize("n,hm", [(65536, 24), (1031, 600)])
+@pytest.mark.parametrize("n,hm", [(65536, 24), (4099, 150)])
 def test_two_streams_one_plan_own_workspaces(n, hm):
     import torch
 
