@@ -1,6 +1,7 @@
 // Launch descriptors shared by the host planner (plan.cpp) and the CUDA
 // kernels.  Plain structs passed by value as kernel parameters.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -256,6 +257,35 @@ struct FourStepLaunch {
   TwoLevel post;     // W_n^{column * k} on the outputs when post.n != 0
 };
 bool fourstep_pass_supported(int nl);
+
+// Dense-batch four-step passes moved by the TMA engine (fourstep_ring.cu):
+// persistent CTAs over `tiles` = members * blocks tiles of c sub-transforms,
+// a ring of `slots` shared-memory slots.  Pass 0: tile (m, b) is columns
+// [b c, b c + c) of member m, loaded and stored through the tensor maps
+// tm_in / tm_out (dims {n2, n1, members}), W_n^{col k} applied (post);
+// pass 1: tile (m, b) is rows [b c, b c + c) of member m (nl contiguous
+// elements each, from `in` with member distance idist), stored transposed
+// through tm_out (dims {n1, n2, members}).
+struct alignas(64) FourStepRingLaunch {
+  CUtensorMap tm_in;   // pass 0 input
+  CUtensorMap tm_out;  // output of either pass
+  const float2* in;    // pass 1 input
+  int64_t tiles, blocks;
+  int64_t idist;
+  int slots;
+  float scale;
+  const float2* tw;  // stage twiddles of length nl
+  TwoLevel post;     // pass 0 only (pass 1: l = 1)
+  int* err;          // host-mapped status word: set to 1 if a bounded device wait ran out
+  uint64_t wait_ns;  // limit of each bounded wait (0: kWaitLimitNs)
+};
+bool fourstep_ring_supported(int nl, int c);
+int fourstep_ring_smem(int nl, int c, int slots);
+cudaError_t launch_fourstep_ring(int nl, int c, int dir, int pass, const FourStepRingLaunch& L, cudaStream_t st);
+// 3-D tensor map over 8-byte elements: dims {d0, d1, d2}, byte strides of
+// dims 1 and 2, box {b0, b1, 1}, shared-memory swizzle for b0*8-byte rows
+cudaError_t encode_tensor_map_c64(CUtensorMap* map, const void* base, uint64_t d0, uint64_t d1, uint64_t d2,
+                                  uint64_t stride1_bytes, uint64_t stride2_bytes, uint32_t b0, uint32_t b1);
 int fourstep_pass_e(int nl);
 int fourstep_pass_smem(int nl, int c);
 cudaError_t launch_fourstep_pass(int nl, int dir, const FourStepLaunch& L, cudaStream_t st);

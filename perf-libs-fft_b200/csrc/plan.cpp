@@ -425,26 +425,72 @@ int64_t four_step_split(int64_t n) {
 
 // power-of-two four-step: both passes are static register kernels
 // (fourstep.cu); members are processed in chunks whose intermediate stays
-// near L2 size
+// near L2 size.  Dense batches (unit strides, 16-byte aligned members) run
+// the bulk-copy ring passes of fourstep_ring.cu instead.
 struct C2CFourStepPow2Node : Node {
   int64_t n = 0, n1 = 0, n2 = 0, chunk = 1;
   int dir = -1;
   Layout lay{};
   FourStepLaunch p1{}, p2{};
   DevBuf tw1, tw2, lo, hi;
+  // ring form: tile widths and slots of each pass (c1 = 0: not used)
+  int c1 = 0, c2 = 0, slots1 = 3, slots2 = 3;
+  HostWord status;
+  void status_words(std::vector<int*>& out) const override { out.push_back(status.p); }
   size_t workspace() const override { return size_t(chunk) * size_t(n) * sizeof(float2); }
   int launches() const override { return int(2 * ((lay.howmany + chunk - 1) / chunk)); }
+  bool ring_ok(const void* in, const void* out) const {
+    return c1 > 0 && lay.istride == 1 && lay.ostride == 1 && lay.idist % 2 == 0 && lay.odist % 2 == 0 &&
+           reinterpret_cast<uintptr_t>(in) % 16 == 0 && reinterpret_cast<uintptr_t>(out) % 16 == 0;
+  }
   cudaError_t run(const void* in, void* out, void* ws, cudaStream_t st) const override {
     const float2* x = static_cast<const float2*>(in);
     float2* y = static_cast<float2*>(out);
     float2* s = static_cast<float2*>(ws);
+    const bool ring = ring_ok(in, out) && reinterpret_cast<uintptr_t>(ws) % 16 == 0;
     for (int64_t m0 = 0; m0 < lay.howmany; m0 += chunk) {
       const int64_t cnt = std::min(chunk, lay.howmany - m0);
+      cudaError_t e;
+      if (ring) {
+        const uint32_t r1 = uint32_t(std::min<int64_t>(n1, 256)), r2 = uint32_t(std::min<int64_t>(n2, 256));
+        FourStepRingLaunch a{};
+        FourStepRingLaunch b{};
+        e = encode_tensor_map_c64(&a.tm_in, x + m0 * lay.idist, uint64_t(n2), uint64_t(n1), uint64_t(cnt),
+                                  uint64_t(n2) * 8u, uint64_t(lay.idist) * 8u, uint32_t(c1), r1);
+        if (e == cudaSuccess)
+          e = encode_tensor_map_c64(&a.tm_out, s, uint64_t(n2), uint64_t(n1), uint64_t(cnt), uint64_t(n2) * 8u,
+                                    uint64_t(n) * 8u, uint32_t(c1), r1);
+        if (e == cudaSuccess)
+          e = encode_tensor_map_c64(&b.tm_out, y + m0 * lay.odist, uint64_t(n1), uint64_t(n2), uint64_t(cnt),
+                                    uint64_t(n1) * 8u, uint64_t(lay.odist) * 8u, uint32_t(c2), r2);
+        if (e != cudaSuccess) return e;
+        a.blocks = n2 / c1;
+        a.tiles = cnt * a.blocks;
+        a.slots = slots1;
+        a.scale = 1.f;
+        a.tw = p1.tw;
+        a.post = p1.post;
+        a.err = status.device();
+        e = launch_fourstep_ring(int(n1), c1, dir, 0, a, st);
+        if (e != cudaSuccess) return e;
+        b.in = s;
+        b.idist = n;
+        b.blocks = n1 / c2;
+        b.tiles = cnt * b.blocks;
+        b.slots = slots2;
+        b.scale = p2.scale;
+        b.tw = p2.tw;
+        b.post = TwoLevel{nullptr, nullptr, 0, 1};
+        b.err = status.device();
+        e = launch_fourstep_ring(int(n2), c2, dir, 1, b, st);
+        if (e != cudaSuccess) return e;
+        continue;
+      }
       FourStepLaunch a = p1;
       a.in = x + m0 * lay.idist;
       a.out = s;
       a.count = cnt * n2;
-      cudaError_t e = launch_fourstep_pass(int(n1), dir, a, st);
+      e = launch_fourstep_pass(int(n1), dir, a, st);
       if (e != cudaSuccess) return e;
       FourStepLaunch b = p2;
       b.in = s;
@@ -458,10 +504,29 @@ struct C2CFourStepPow2Node : Node {
   std::string describe() const override {
     std::ostringstream o;
     o << "(c2c-four-step-pow2 n=" << n << " " << n1 << "x" << n2 << " chunk=" << chunk << " c=" << p1.c << "/"
-      << p2.c << ")";
+      << p2.c;
+    if (c1) o << " bulk-ring c=" << c1 << "/" << c2 << " slots=" << slots1 << "/" << slots2;
+    o << ")";
     return o.str();
   }
 };
+
+// ring-pass shape for a sub-transform length and pass: tile width and slots
+// (PLFFT_B200_FSR_C / _SLOTS override both passes, _C1 / _S1 and _C2 / _S2
+// one pass), the slots reduced to fit
+static bool fourstep_ring_shape(int nl, int pass, int& c, int& slots) {
+  // measured best at 2^14..2^20: 8-column tiles; two slots (more CTAs per
+  // SM) up to nl = 256, three above
+  c = 8;
+  slots = nl <= 256 ? 2 : 3;
+  c = env_int("PLFFT_B200_FSR_C", c);
+  slots = env_int("PLFFT_B200_FSR_SLOTS", slots);
+  c = env_int(pass == 0 ? "PLFFT_B200_FSR_C1" : "PLFFT_B200_FSR_C2", c);
+  slots = env_int(pass == 0 ? "PLFFT_B200_FSR_S1" : "PLFFT_B200_FSR_S2", slots);
+  if (!fourstep_ring_supported(nl, c)) return false;
+  while (slots > 2 && fourstep_ring_smem(nl, c, slots) > 220 * 1024) --slots;
+  return slots >= 2 && fourstep_ring_smem(nl, c, slots) <= 220 * 1024;
+}
 
 static int fourstep_c(int nl) {
   const int t = nl / fourstep_pass_e(nl);
@@ -470,8 +535,11 @@ static int fourstep_c(int nl) {
   return c;
 }
 
+// ring_shape: {c1, slots1, c2, slots2} of the bulk-copy ring passes (all 0:
+// the defaults); c_override selects the per-element passes with that width
 static std::unique_ptr<Node> make_four_step_pow2(int64_t n, const Layout& lay, int dir, float scale,
-                                                 int c_override = 0, int chunk_mb = 0) {
+                                                 int c_override = 0, int chunk_mb = 0,
+                                                 const int* ring_shape = nullptr) {
   if (!is_pow2(n) || std::getenv("PLFFT_B200_NO_FS_POW2")) return nullptr;
   int b = ilog2(n);
   const int64_t n1 = int64_t(1) << (b / 2), n2 = n / n1;
@@ -513,6 +581,27 @@ static std::unique_ptr<Node> make_four_step_pow2(int64_t n, const Layout& lay, i
   node->p2 = FourStepLaunch{nullptr, nullptr, 0, n1, n, n2, 1, lay.odist, lay.ostride, n1 * lay.ostride,
                             c_override ? c_override : fourstep_c(int(n2)), scale, node->tw2.as<float2>(),
                             TwoLevel{nullptr, nullptr, 0, 1}};
+  if (node->status.alloc() != cudaSuccess) return nullptr;
+  if (!std::getenv("PLFFT_B200_NO_FS_RING") && !c_override && lay.istride == 1 && lay.ostride == 1) {
+    int c1, s1, c2, s2;
+    bool ok = fourstep_ring_shape(int(n1), 0, c1, s1) && fourstep_ring_shape(int(n2), 1, c2, s2);
+    if (ring_shape) {
+      c1 = ring_shape[0];
+      s1 = ring_shape[1];
+      c2 = ring_shape[2];
+      s2 = ring_shape[3];
+      ok = fourstep_ring_supported(int(n1), c1) && fourstep_ring_supported(int(n2), c2) &&
+           fourstep_ring_smem(int(n1), c1, s1) <= 220 * 1024 && fourstep_ring_smem(int(n2), c2, s2) <= 220 * 1024 &&
+           s1 >= 2 && s2 >= 2 && s1 <= 4 && s2 <= 4;
+      if (!ok) return nullptr;
+    }
+    if (ok && n2 % c1 == 0 && n1 % c2 == 0) {
+      node->c1 = c1;
+      node->c2 = c2;
+      node->slots1 = s1;
+      node->slots2 = s2;
+    }
+  }
   return node;
 }
 
@@ -836,6 +925,19 @@ std::vector<std::unique_ptr<Node>> make_c2c_candidates(int64_t n, const Layout& 
         if (level < 3 && mb != 512) continue;
         if (auto f = make_four_step_pow2(n, lay, dir, scale, c, mb)) out.push_back(std::move(f));
       }
+    // shapes of the bulk-copy ring passes (dense batches)
+    if (unit) {
+      const int64_t n1 = int64_t(1) << (ilog2(n) / 2), n2 = n / n1;
+      auto shapes = [](int64_t nl) {
+        return nl <= 512 ? std::vector<std::pair<int, int>>{{8, 2}, {8, 3}, {16, 3}}
+                         : std::vector<std::pair<int, int>>{{8, 3}, {4, 2}, {4, 3}};
+      };
+      for (const auto& a : shapes(n1))
+        for (const auto& b : shapes(n2)) {
+          const int rs[4] = {a.first, a.second, b.first, b.second};
+          if (auto f = make_four_step_pow2(n, lay, dir, scale, 0, 0, rs)) out.push_back(std::move(f));
+        }
+    }
   }
   // drop duplicates of the default (same description)
   std::vector<std::unique_ptr<Node>> uniq;

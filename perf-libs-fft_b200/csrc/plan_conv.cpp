@@ -265,10 +265,15 @@ int64_t next_pow2(int64_t v) {
 
 }  // namespace
 
+// the reference planner's choice (src/planner/planner.cpp:49-182,
+// src/planner/strategies/rader.hpp:816-856): Rader for a prime whose p - 1
+// needs no convolution itself, Bluestein for every other non-smooth length
+static bool use_rader(int64_t n) { return n > 2 && is_prime(n) && is_smooth(n - 1); }
+
 int64_t conv_fused_length(int64_t n) {
   if (n < 3) return 0;
   // Rader convolves l = n - 1 terms, Bluestein n: a cyclic length >= 2l - 1
-  const int64_t m = next_pow2(std::max<int64_t>(64, is_prime(n) ? 2 * n - 3 : 2 * n - 1));
+  const int64_t m = next_pow2(std::max<int64_t>(64, use_rader(n) ? 2 * n - 3 : 2 * n - 1));
   return m <= 8192 ? m : 0;
 }
 
@@ -279,7 +284,7 @@ std::unique_ptr<Node> make_conv_fused(int64_t n, const Layout& lay, int dir, flo
   if (std::getenv("PLFFT_B200_CONV_UNFUSED")) return nullptr;
   const int64_t m = conv_fused_length(n);
   if (m == 0) return nullptr;
-  const bool rader = is_prime(n);
+  const bool rader = use_rader(n);
   const auto shapes = conv_fused_shapes(int(m));
   if (shapes.empty()) return nullptr;
   int e = shapes[0].first, minb = shapes[0].second;
@@ -351,11 +356,11 @@ std::unique_ptr<Node> make_conv_fused(int64_t n, const Layout& lay, int dir, flo
   return node;
 }
 
-// Strategy: lengths whose convolution fits a power-of-two m <= 8192 run as
-// one fused launch (Rader for every prime, since its m never exceeds
-// Bluestein's); longer ones follow the reference planner's rule (Rader for
-// prime n with smooth n - 1, else Bluestein over the smallest smooth
-// m >= 2n - 1) with multi-launch length-m C2C plans.
+// Strategy (the reference planner's rule): Rader for prime n with smooth
+// n - 1, else Bluestein.  Lengths whose convolution fits a power-of-two
+// m <= 8192 run as one fused launch; longer ones convolve over m = n - 1
+// (Rader) or the smallest smooth m >= 2n - 1 (Bluestein) with multi-launch
+// length-m C2C plans.
 std::unique_ptr<Node> make_conv_node(int64_t n, const Layout& lay, int dir, float scale, std::string* why) {
   if (auto f = make_conv_fused(n, lay, dir, scale, why, 0, 0, 0)) return f;
   auto node = std::make_unique<ConvNode>();
@@ -363,7 +368,7 @@ std::unique_ptr<Node> make_conv_node(int64_t n, const Layout& lay, int dir, floa
   node->n = n;
   node->lay = lay;
   node->scale = scale;
-  node->rader = is_prime(n) && is_smooth(n - 1) && n > 2;
+  node->rader = use_rader(n);
   node->m = node->rader ? n - 1 : next_smooth(2 * n - 1);
   const int64_t m = node->m;
   const int64_t target = 64ll << 20;

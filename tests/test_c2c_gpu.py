@@ -52,14 +52,15 @@ def test_c2c_reference_conv_layouts(case, direction):
     assert oracle.rel_l2(got, ref) <= oracle.fp32_tol(n), plan.describe()
 
 
-# (n, schedule): one fused launch while the convolution fits a power-of-two
-# m <= 8192 (Rader for every prime p <= 4097: m >= 2p - 3; Bluestein for
-# other lengths n <= 4096: m >= 2n - 1), multi-launch convolutions beyond
-CONV_CASES = [(17, "rader-fused"), (23, "rader-fused"), (47, "rader-fused"), (97, "rader-fused"),
-              (1009, "rader-fused"), (1031, "rader-fused"), (4093, "rader-fused"), (94, "bluestein-fused"),
-              (1034, "bluestein-fused"),
-              (1058, "bluestein-fused"), (2870, "bluestein-fused"), (4094, "bluestein-fused"),
-              (4099, "(bluestein n="), (2 * 8191, "(bluestein n="), (65537, "(rader n="), (8191 * 3, "(bluestein n=")]
+# (n, schedule): Rader for primes p with smooth p - 1, Bluestein otherwise
+# (the reference planner's rule); one fused launch while the convolution fits
+# a power-of-two m <= 8192 (Rader: m >= 2p - 3, Bluestein: m >= 2n - 1),
+# multi-launch convolutions beyond
+CONV_CASES = [(17, "rader-fused"), (23, "rader-fused"), (97, "rader-fused"), (1009, "rader-fused"),
+              (4001, "rader-fused"), (47, "bluestein-fused"), (94, "bluestein-fused"), (1031, "bluestein-fused"),
+              (1058, "bluestein-fused"), (2870, "bluestein-fused"), (4093, "bluestein-fused"),
+              (4094, "bluestein-fused"), (4099, "(bluestein n="), (2 * 8191, "(bluestein n="), (65537, "(rader n="),
+              (8191 * 3, "(bluestein n=")]
 
 
 @pytest.mark.parametrize("n,expect", CONV_CASES)
@@ -76,7 +77,8 @@ def test_c2c_rader_bluestein(n, expect, direction):
 # filled), strided members
 @pytest.mark.parametrize("e,minb", [(16, 2), (16, 3), (16, 4), (32, 2)])
 @pytest.mark.parametrize("n,hm,layout", [(17, 37, (1, 17, 1, 17)), (1009, 11, (1, 1009, 1, 1009)),
-                                         (1034, 9, (9, 1, 9, 1)), (4093, 5, (1, 4093, 1, 4093)),
+                                         (1031, 9, (9, 1, 9, 1)), (4093, 5, (1, 4093, 1, 4093)),
+                                         (4001, 3, (1, 4003, 1, 4001)), (3001, 4, (3, 9003, 1, 3001)),
                                          (300 * 7 - 1, 4, (1, 2099, 1, 2100)), (263, 33, (2, 600, 1, 263))])
 def test_c2c_conv_fused_shapes(monkeypatch, e, minb, n, hm, layout):
     monkeypatch.setenv("PLFFT_B200_CONV_E", str(e))
@@ -94,6 +96,32 @@ def test_c2c_four_step(n):
     howmany = 2
     got, ref, plan = c2c_case(n, howmany, seed=3, method="fft")
     assert "four-step" in plan.describe()
+    assert oracle.rel_l2(got, ref) <= oracle.fp32_tol(n), plan.describe()
+
+
+# the bulk-copy ring passes (dense batches): every supported tile width and
+# slot count, both directions, more tiles than CTAs so each CTA's ring wraps
+@pytest.mark.parametrize("n,c,slots", [(1 << 14, 16, 3), (1 << 15, 8, 2), (1 << 16, 16, 3), (1 << 16, 16, 2),
+                                       (1 << 16, 8, 3), (1 << 17, 16, 3), (1 << 18, 8, 3), (1 << 19, 8, 3),
+                                       (1 << 20, 8, 2), (1 << 20, 4, 3)])
+def test_c2c_four_step_ring(monkeypatch, n, c, slots):
+    import plfft
+
+    monkeypatch.setenv("PLFFT_B200_FSR_C", str(c))
+    monkeypatch.setenv("PLFFT_B200_FSR_SLOTS", str(slots))
+    howmany = max(2, (1 << 22) // n)
+    for direction in (-1, 1):
+        got, ref, plan = c2c_case(n, howmany, direction=direction, seed=n + c, method="fft")
+        assert "bulk-ring" in plan.describe(), plan.describe()
+        assert oracle.rel_l2(got, ref) <= oracle.fp32_tol(n), plan.describe()
+
+
+# strided or unaligned members keep the per-element four-step passes
+@pytest.mark.parametrize("case", [(1 << 16, 3, 1, 65537, 1, 65536), (1 << 16, 2, 2, 2 * 65536, 1, 65536)])
+def test_c2c_four_step_strided(case):
+    n, hm, is_, id_, os_, od = case
+    got, ref, plan = c2c_case(n, hm, is_, id_, os_, od, seed=5, method="fft")
+    assert "four-step" in plan.describe(), plan.describe()
     assert oracle.rel_l2(got, ref) <= oracle.fp32_tol(n), plan.describe()
 
 
