@@ -105,6 +105,22 @@ plfft_status_t plfft_cuda_group_create(plfft_cuda_group_t **group,
 plfft_status_t plfft_cuda_group_execute_async(plfft_cuda_group_t *group,
                                               const void *d_input,
                                               void *d_output, void *stream);
+/* plfft_cuda_group_create with a planner rigor (reference include/plfft.h:
+ * 192-201 semantics).  PLFFT_ESTIMATE is plfft_cuda_group_create (its
+ * default schedule).  MEASURE, PATIENT and EXHAUSTIVE build candidate
+ * schedules of the group (four-step tile width, same-length transforms
+ * merged into one task, largest radix; 4, 6 and 10 candidates), time each on scratch device buffers of the
+ * group's spans within 0.1 / 0.5 / 2 s of timed work, keep the fastest and
+ * remember it in the wisdom (plfft_cuda_wisdom_*), keyed by the lengths,
+ * offsets, direction and device.  Returns PLFFT_INVALID_PLANNER_RIGOR for
+ * other rigor values. */
+plfft_status_t plfft_cuda_group_create_tuned(plfft_cuda_group_t **group,
+                                             int64_t count,
+                                             const int64_t *lengths,
+                                             const int64_t *in_offsets,
+                                             const int64_t *out_offsets,
+                                             plfft_direction_t direction,
+                                             plfft_rigor_t rigor);
 int plfft_cuda_group_get_launch_count(const plfft_cuda_group_t *group);
 plfft_status_t plfft_cuda_group_describe(const plfft_cuda_group_t *group,
                                          char *buf, size_t len);

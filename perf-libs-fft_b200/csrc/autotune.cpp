@@ -126,6 +126,10 @@ double time_node(const Node& node, const void* in, void* out, void* ws, cudaStre
 
 }  // namespace
 
+bool wisdom_recall(const std::string& key, std::string& choice) { return recall(key, choice); }
+void wisdom_remember(const std::string& key, const std::string& choice) { remember(key, choice); }
+std::string wisdom_device() { return device_name(); }
+
 std::string wisdom_key(const ConfigData& c) {
   static const char* kinds[] = {"c2c", "r2c", "c2r", "r2r"};
   std::ostringstream o;

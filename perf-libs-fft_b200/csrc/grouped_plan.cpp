@@ -19,6 +19,7 @@
 // CUDA graph per (input, output) pointer pair and replayed.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <sstream>
@@ -48,9 +49,26 @@ struct Tables {
 
 }  // namespace
 
+// Schedule of a grouped execution (the autotuner's choices): columns or rows
+// per four-step tile, same-length on-chip transforms merged into one task,
+// largest radix of the on-chip stage lists.
+struct GroupShape {
+  // measured on the 4000-transform mix: 32-wide tiles 1.15x over 16, 8 at
+  // 0.77x; merging 1.02x; radix 8 or 32 below 16
+  int tile_cap = 32;
+  int merge_cap = 16;
+  int max_radix = 16;
+  std::string str() const {
+    std::ostringstream o;
+    o << "tile=" << tile_cap << " merge=" << merge_cap << " radix=" << max_radix;
+    return o.str();
+  }
+};
+
 struct GroupData {
   int device = 0;
   int dir = -1;
+  GroupShape shape;
   int64_t count = 0;
   std::vector<GTask> tasks[kPhases];
   DevBuf tasks_dev[kPhases];
@@ -81,7 +99,7 @@ struct GroupData {
     auto it = desc_of.find(L);
     if (it != desc_of.end()) return it->second;
     std::vector<float2> tw;
-    const FftDesc d = make_desc(L, factor_radices(L, 16), tw);
+    const FftDesc d = make_desc(L, factor_radices(L, shape.max_radix), tw);
     auto buf = std::make_unique<DevBuf>();
     if (buf->upload(tw) != cudaSuccess) return -1;
     descs.push_back(d);
@@ -93,13 +111,13 @@ struct GroupData {
 
   bool onchip(int64_t L, int cnt = 1) {
     if (L > kGroupOnChip || !is_smooth(L)) return false;
-    return tile_fits(int(L), cnt, factor_radices(L, 16));
+    return tile_fits(int(L), cnt, factor_radices(L, shape.max_radix));
   }
 
   // largest tile count that fits for length L (up to cap)
   int tile_count(int L, int cap) {
     int c = cap;
-    while (c > 1 && !tile_fits(L, c, factor_radices(L, 16))) --c;
+    while (c > 1 && !tile_fits(L, c, factor_radices(L, shape.max_radix))) --c;
     return c;
   }
 
@@ -213,7 +231,7 @@ struct GroupData {
     const int d1 = desc(int(m1)), d2 = desc(int(m2));
     if (d1 < 0 || d2 < 0) return false;
     const TwoLevel tl = two_level(m);
-    const int c1 = tile_count(int(m1), 16), c2 = tile_count(int(m2), 16);
+    const int c1 = tile_count(int(m1), shape.tile_cap), c2 = tile_count(int(m2), shape.tile_cap);
     for (int64_t col0 = 0; col0 < m2; col0 += c1) {
       GTask T = base_task(GT_TILE, tdir, int(m1), int(std::min<int64_t>(c1, m2 - col0)), d1);
       T.in_buf = in_buf;
@@ -314,17 +332,30 @@ struct GroupData {
       const int64_t n = lengths[i];
       const Plan& pl = plans[i];
       if (pl.kind == 0) {
-        GTask T = base_task(GT_TILE, dir, int(n), 1, desc(int(n)));
+        // transforms i, i+1, ... of the same length whose offsets step by
+        // the same distances (>= n, so members do not overlap) share a task
+        int run = 1;
+        if (shape.merge_cap > 1) {
+          const int cap = tile_count(int(n), shape.merge_cap);
+          const int64_t di = i + 1 < cnt ? in_offs[i + 1] - in_offs[i] : 0;
+          const int64_t dout = i + 1 < cnt ? out_offs[i + 1] - out_offs[i] : 0;
+          while (run < cap && i + run < cnt && plans[i + run].kind == 0 && lengths[i + run] == n &&
+                 in_offs[i + run] - in_offs[i + run - 1] == di && out_offs[i + run] - out_offs[i + run - 1] == dout &&
+                 di >= n && dout >= n)
+            ++run;
+        }
+        GTask T = base_task(GT_TILE, dir, int(n), run, desc(int(n)));
         T.in_buf = 0;
         T.in_off = in_offs[i];
         T.ikstride = 1;
-        T.icdist = n;
+        T.icdist = run > 1 ? in_offs[i + 1] - in_offs[i] : n;
         T.out_buf = 1;
         T.out_off = out_offs[i];
         T.okstride = 1;
-        T.ocdist = n;
+        T.ocdist = run > 1 ? out_offs[i + 1] - out_offs[i] : n;
         tasks[0].push_back(T);
-        ++nonchip;
+        nonchip += run;
+        i += run - 1;
       } else if (pl.kind == 1) {
         Tables* t = rader_tables(n);
         GTask T = base_task(GT_RADER, dir, int(pl.m), 1, desc(int(pl.m)));
@@ -478,7 +509,7 @@ struct GroupData {
 
   std::string describe() const {
     std::ostringstream o;
-    o << "(group count=" << count << " onchip=" << nonchip << " rader=" << nrader << " bluestein=" << nblue
+    o << "(group count=" << count << " " << shape.str() << " onchip=" << nonchip << " rader=" << nrader << " bluestein=" << nblue
       << " four-step=" << nlarge << " long-conv=" << nconv_large << " phases=" << launches() << " tasks=["
       << tasks[0].size() << "," << tasks[1].size() << "," << tasks[2].size() << "," << tasks[3].size()
       << "] smem=" << smem_bytes << " graph=" << (use_graph ? 1 : 0) << ")";
@@ -510,6 +541,15 @@ plfft_status_t plfft_cuda_group_create(plfft_cuda_group_t** group, int64_t count
   cudaGetDevice(&h->g.device);
   h->g.dir = int(direction);
   h->g.use_graph = std::getenv("PLFFT_B200_GROUP_NOGRAPH") == nullptr;
+  // PLFFT_B200_GROUP_SHAPE=tile,merge,radix: a schedule other than the default
+  if (const char* v = std::getenv("PLFFT_B200_GROUP_SHAPE")) {
+    int a = 0, b = 0, c = 0;
+    if (std::sscanf(v, "%d,%d,%d", &a, &b, &c) == 3 && a >= 1 && b >= 1 && (c == 8 || c == 16 || c == 32)) {
+      h->g.shape.tile_cap = a;
+      h->g.shape.merge_cap = b;
+      h->g.shape.max_radix = c;
+    }
+  }
   if (!h->g.build(count, lengths, in_offsets, out_offsets)) {
     delete h;
     return PLFFT_PLAN_CREATION_FAILED;
@@ -523,6 +563,142 @@ plfft_status_t plfft_cuda_group_execute_async(plfft_cuda_group_t* group, const v
   if (!group || !d_input || !d_output) return PLFFT_NULL_ARGUMENT;
   const cudaError_t e = group->g.execute(d_input, d_output, static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? PLFFT_OK : PLFFT_CUDA_ERROR;
+}
+
+plfft_status_t plfft_cuda_group_create_tuned(plfft_cuda_group_t** group, int64_t count, const int64_t* lengths,
+                                             const int64_t* in_offsets, const int64_t* out_offsets,
+                                             plfft_direction_t direction, plfft_rigor_t rigor) {
+  if (rigor == PLFFT_ESTIMATE) return plfft_cuda_group_create(group, count, lengths, in_offsets, out_offsets, direction);
+  if (!group) return PLFFT_NULL_ARGUMENT;
+  *group = nullptr;
+  if (!lengths || !in_offsets || !out_offsets) return PLFFT_NULL_ARGUMENT;
+  if (count < 1) return PLFFT_UNSUPPORTED_BATCH;
+  if (direction != PLFFT_FORWARD && direction != PLFFT_BACKWARD) return PLFFT_INVALID_TRANSFORM_KIND;
+  if (rigor != PLFFT_MEASURE && rigor != PLFFT_PATIENT && rigor != PLFFT_EXHAUSTIVE) return PLFFT_INVALID_PLANNER_RIGOR;
+  for (int64_t i = 0; i < count; ++i)
+    if (lengths[i] < 1) return PLFFT_INVALID_SIZE;
+  int device = 0;
+  cudaGetDevice(&device);
+  const bool use_graph = std::getenv("PLFFT_B200_GROUP_NOGRAPH") == nullptr;
+  auto make = [&](const GroupShape& sh) -> plfft_cuda_group_t* {
+    auto* h = new plfft_cuda_group_t;
+    h->g.device = device;
+    h->g.dir = int(direction);
+    h->g.use_graph = use_graph;
+    h->g.shape = sh;
+    if (!h->g.build(count, lengths, in_offsets, out_offsets)) {
+      delete h;
+      return nullptr;
+    }
+    return h;
+  };
+  // candidate schedules, the default first: more at each rigor level
+  std::vector<GroupShape> cands;
+  auto add = [&](int tile, int merge, int radix) {
+    GroupShape sh;
+    sh.tile_cap = tile;
+    sh.merge_cap = merge;
+    sh.max_radix = radix;
+    cands.push_back(sh);
+  };
+  add(32, 16, 16);
+  add(16, 16, 16);
+  add(64, 16, 16);
+  add(32, 1, 16);
+  if (rigor >= PLFFT_PATIENT) {
+    add(32, 16, 8);
+    add(32, 16, 32);
+  }
+  if (rigor >= PLFFT_EXHAUSTIVE) {
+    add(8, 16, 16);
+    add(16, 1, 16);
+    add(32, 64, 16);
+    add(64, 64, 16);
+  }
+  // the problem's key: FNV-1a over lengths and offsets, the count, direction, device
+  uint64_t hsh = 1469598103934665603ull;
+  auto mix = [&](int64_t v) {
+    for (int b = 0; b < 8; ++b) {
+      hsh ^= uint64_t(v >> (8 * b)) & 0xffu;
+      hsh *= 1099511628211ull;
+    }
+  };
+  int64_t in_span = 0, out_span = 0;
+  for (int64_t i = 0; i < count; ++i) {
+    mix(lengths[i]);
+    mix(in_offsets[i]);
+    mix(out_offsets[i]);
+    in_span = std::max(in_span, in_offsets[i] + lengths[i]);
+    out_span = std::max(out_span, out_offsets[i] + lengths[i]);
+  }
+  std::ostringstream key;
+  key << "group count=" << count << " hash=" << std::hex << hsh << std::dec << " dir=" << int(direction)
+      << " dev=" << wisdom_device();
+  std::string known;
+  if (wisdom_recall(key.str(), known))
+    for (const GroupShape& sh : cands)
+      if (sh.str() == known) {
+        if (auto* h = make(sh)) {
+          *group = h;
+          return PLFFT_OK;
+        }
+      }
+  // time each candidate on scratch buffers with the group's spans: one
+  // warm-up, then executions until its share of the budget is spent (3 at
+  // least); a challenger replaces the incumbent only if >= 2% faster
+  const double budget = rigor == PLFFT_MEASURE ? 0.1 : (rigor == PLFFT_PATIENT ? 0.5 : 2.0);
+  DevBuf din, dout;
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  const bool scratch = din.alloc(size_t(in_span) * sizeof(float2)) == cudaSuccess &&
+                       dout.alloc(size_t(out_span) * sizeof(float2)) == cudaSuccess &&
+                       cudaMemset(din.p, 0, size_t(in_span) * sizeof(float2)) == cudaSuccess &&
+                       cudaStreamCreate(&st) == cudaSuccess && cudaEventCreate(&e0) == cudaSuccess &&
+                       cudaEventCreate(&e1) == cudaSuccess;
+  plfft_cuda_group_t* best = nullptr;
+  double best_t = -1;
+  if (scratch) {
+    const double share = budget / double(cands.size());
+    for (const GroupShape& sh : cands) {
+      plfft_cuda_group_t* h = make(sh);
+      if (!h) continue;
+      double t = -1;
+      if (h->g.launch_all(din.p, dout.p, st) == cudaSuccess && cudaStreamSynchronize(st) == cudaSuccess) {
+        double spent = 0;
+        int reps = 0;
+        while (reps < 3 || (spent < share && reps < 64)) {
+          cudaEventRecord(e0, st);
+          if (h->g.launch_all(din.p, dout.p, st) != cudaSuccess) break;
+          cudaEventRecord(e1, st);
+          if (cudaEventSynchronize(e1) != cudaSuccess) break;
+          float ms = 0;
+          cudaEventElapsedTime(&ms, e0, e1);
+          const double sec = ms * 1e-3;
+          t = t < 0 ? sec : std::min(t, sec);
+          spent += sec;
+          ++reps;
+        }
+      }
+      cudaGetLastError();
+      if (t > 0 && (best_t < 0 || t < best_t * 0.98)) {
+        delete best;
+        best = h;
+        best_t = t;
+      } else {
+        delete h;
+      }
+    }
+  } else {
+    cudaGetLastError();
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (st) cudaStreamDestroy(st);
+  if (!best) best = make(cands[0]);  // no room or time to measure: the default schedule
+  if (!best) return PLFFT_PLAN_CREATION_FAILED;
+  if (best_t > 0) wisdom_remember(key.str(), best->g.shape.str());
+  *group = best;
+  return PLFFT_OK;
 }
 
 int plfft_cuda_group_get_launch_count(const plfft_cuda_group_t* group) { return group ? group->g.launches() : 0; }

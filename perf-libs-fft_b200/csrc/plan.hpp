@@ -162,6 +162,12 @@ std::unique_ptr<Node> make_c2c_node(int64_t n, const Layout& lay, int dir, float
 std::vector<std::unique_ptr<Node>> make_c2c_candidates(int64_t n, const Layout& lay, int dir, float scale,
                                                        int precision, int level);
 
+// The autotuner's wisdom store (autotune.cpp): problem key -> description
+// of the chosen schedule, with the device name for keys
+bool wisdom_recall(const std::string& key, std::string& choice);
+void wisdom_remember(const std::string& key, const std::string& choice);
+std::string wisdom_device();
+
 // Plan-time autotuning for rigor MEASURE/PATIENT/EXHAUSTIVE (autotune.cpp):
 // times the candidates and remembers the winner in wisdom; note receives
 // "wisdom" or "autotuned k/m candidates".

@@ -138,6 +138,7 @@ _SIGS = [
     ("plfft_cuda_execute_adjoint_async", _INT, [_P, _P, _P, _P, _P]),
     ("plfft_cuda_plan_get_adjoint_workspace_size", _INT, [_P, ctypes.POINTER(ctypes.c_size_t)]),
     ("plfft_cuda_group_create", _INT, [_PP, _I64, _P, _P, _P, _INT]),
+    ("plfft_cuda_group_create_tuned", _INT, [_PP, _I64, _P, _P, _P, _INT, _INT]),
     ("plfft_cuda_group_execute_async", _INT, [_P, _P, _P, _P]),
     ("plfft_cuda_group_get_launch_count", _INT, [_P]),
     ("plfft_cuda_group_describe", _INT, [_P, ctypes.c_char_p, ctypes.c_size_t]),
@@ -319,16 +320,22 @@ def c2c_execute_noalloc(d_in, d_out, n, howmany, direction=FORWARD, stream=0):
 class Group:
     """plfft_cuda_group_t: many C2C transforms of different lengths in one grouped execution."""
 
-    def __init__(self, lengths, in_offsets, out_offsets, direction=FORWARD):
+    def __init__(self, lengths, in_offsets, out_offsets, direction=FORWARD, rigor=None):
         import numpy as np
 
         self._len = np.ascontiguousarray(lengths, dtype=np.int64)
         self._io = np.ascontiguousarray(in_offsets, dtype=np.int64)
         self._oo = np.ascontiguousarray(out_offsets, dtype=np.int64)
         h = ctypes.c_void_p()
-        st = lib().plfft_cuda_group_create(ctypes.byref(h), len(self._len), self._len.ctypes.data,
-                                           self._io.ctypes.data, self._oo.ctypes.data, int(direction))
-        _check(st, "plfft_cuda_group_create")
+        if rigor is None:
+            st = lib().plfft_cuda_group_create(ctypes.byref(h), len(self._len), self._len.ctypes.data,
+                                               self._io.ctypes.data, self._oo.ctypes.data, int(direction))
+            _check(st, "plfft_cuda_group_create")
+        else:
+            st = lib().plfft_cuda_group_create_tuned(ctypes.byref(h), len(self._len), self._len.ctypes.data,
+                                                     self._io.ctypes.data, self._oo.ctypes.data, int(direction),
+                                                     int(rigor))
+            _check(st, "plfft_cuda_group_create_tuned")
         self.handle = h
 
     def execute_async(self, d_in, d_out, stream=0):

@@ -13,7 +13,7 @@ import plfft
 pytestmark = pytest.mark.gpu
 
 
-def _run_group(lengths, direction, seed, gap=0):
+def _run_group(lengths, direction, seed, gap=0, rigor=None):
     import torch
 
     lengths = np.asarray(lengths, np.int64)
@@ -21,7 +21,7 @@ def _run_group(lengths, direction, seed, gap=0):
     total = int(offs[-1] + lengths[-1])
     rng = np.random.default_rng(seed)
     x = (rng.uniform(-1, 1, total) + 1j * rng.uniform(-1, 1, total)).astype(np.complex64)
-    g = plfft.Group(lengths, offs, offs, direction)
+    g = plfft.Group(lengths, offs, offs, direction, rigor=rigor)
     d_in = torch.from_numpy(x).cuda()
     d_out = torch.zeros(total, dtype=torch.complex64, device="cuda")
     g.execute_async(d_in.data_ptr(), d_out.data_ptr())
@@ -79,3 +79,39 @@ def test_group_synthetic_mix_sample():
     rng = np.random.default_rng(0)
     pick = rng.choice(len(lengths), 40, replace=False)
     _check([lengths[i] for i in pick], x, y, [offs[i] for i in pick], -1)
+
+
+# the schedule shapes the grouped autotuner chooses from: four-step tile
+# width, same-length on-chip transforms merged into one task (runs of equal
+# lengths with equal offset steps), largest radix of the stage lists
+SHAPE_LENGTHS = ([64] * 40 + [1000] * 9 + [17] * 3 + [4096] * 5 + [8192] * 3 + [16384] * 2 +
+                 [12289, 9001, 1031, 97, 6561, 6561])
+
+
+@pytest.mark.parametrize("gap", [0, 3])
+@pytest.mark.parametrize("shape", ["16,1,16", "8,16,8", "32,64,32", "64,16,16", "16,4,16"])
+def test_group_shapes(monkeypatch, shape, gap):
+    monkeypatch.setenv("PLFFT_B200_GROUP_SHAPE", shape)
+    g, x, y, offs = _run_group(SHAPE_LENGTHS, -1, seed=5, gap=gap)
+    t, m, r = shape.split(",")
+    assert "tile=%s merge=%s radix=%s" % (t, m, r) in g.describe(), g.describe()
+    _check(SHAPE_LENGTHS, x, y, offs, -1)
+
+
+def test_group_tuned_and_wisdom():
+    """MEASURE rigor times candidate schedules and keeps the fastest; a second
+    group of the same problem takes the choice from the wisdom."""
+    from helpers import grouped_lengths
+
+    plfft.wisdom_forget()
+    lengths = grouped_lengths(120, seed=11, max_len=20000)
+    g, x, y, offs = _run_group(lengths, 1, seed=6, rigor=plfft.Rigor.MEASURE)
+    d = g.describe()
+    assert "tile=" in d, d
+    pick = np.random.default_rng(1).choice(len(lengths), 20, replace=False)
+    _check([lengths[i] for i in pick], x, y, [offs[i] for i in pick], 1)
+    g2, x2, y2, offs2 = _run_group(lengths, 1, seed=7, rigor=plfft.Rigor.MEASURE)
+    assert g2.describe() == d
+    _check([lengths[i] for i in pick], x2, y2, [offs2[i] for i in pick], 1)
+    with pytest.raises(plfft.PlfftError):
+        _run_group([16, 32], -1, seed=8, rigor=7)
