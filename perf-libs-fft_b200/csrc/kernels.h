@@ -125,6 +125,21 @@ struct RealWrapLaunch {
 };
 cudaError_t launch_realwrap(bool pre, int kind, const RealWrapLaunch& L, int64_t m0, int64_t cnt,
                             cudaStream_t st);
+// Half-length R2C / C2R (realwrap.cu) for even n = 2m, FP32: the split after
+// (R2C) or the merge before (C2R) a length-m C2C over the member's real data
+// read as complex pairs.  Distances and strides in complex elements of the
+// complex side; work holds m complex per member of the chunk.
+struct RealHalfLaunch {
+  const float2* in;  // C2R: the complex input
+  float2* out;       // R2C: the complex output
+  float2* work;      // [chunk][m]
+  int64_t m;
+  int64_t istride, idist, ostride, odist;
+  float scale;
+  int wmode_in, wmode_out;  // AdjointWeight modes over the n-point spectrum
+  const float2* tw;         // W_n^k, k = 0..m
+};
+cudaError_t launch_real_half(bool r2c, const RealHalfLaunch& L, int64_t m0, int64_t cnt, cudaStream_t st);
 
 // Rader / Bluestein elementwise passes (conv.cu).  n: transform length,
 // m: convolution length (M for Bluestein, P-1 for Rader).

@@ -86,10 +86,134 @@ int wrap_dir(int kind) {
   }
 }
 
+// R2C / C2R of even n = 2m through a length-m C2C over the real data read as
+// complex pairs (realwrap.cu, launch_real_half): R2C = C2C in place of the
+// user's input into work, then the split; C2R = the merge into work, then the
+// C2C into the user's output.  Members whose real side is not 8-byte aligned
+// (odd real distance or base) run the generic full-length node instead.
+struct RealHalfNode : Node {
+  bool r2c = true;
+  int64_t n = 0, m = 0, chunk = 1;
+  Layout lay{};
+  float scale = 1.f;
+  int wmode_in = AW_NONE, wmode_out = AW_NONE;
+  DevBuf tw;
+  std::unique_ptr<Node> inner, inner_last;  // `chunk` members, and the last chunk's remainder
+  std::unique_ptr<Node> generic;
+  void status_words(std::vector<int*>& out) const override {
+    inner->status_words(out);
+    if (inner_last) inner_last->status_words(out);
+    generic->status_words(out);
+  }
+  size_t work_bytes() const { return (size_t(chunk) * size_t(m) * sizeof(float2) + 255) & ~size_t(255); }
+  size_t workspace() const override {
+    size_t iw = inner->workspace();
+    if (inner_last) iw = std::max(iw, inner_last->workspace());
+    return std::max(work_bytes() + iw, generic->workspace());
+  }
+  int launches() const override {
+    const int64_t chunks = (lay.howmany + chunk - 1) / chunk;
+    return int(chunks * (1 + inner->launches()));
+  }
+  bool paired(const void* real_side, int64_t real_dist) const {
+    return reinterpret_cast<uintptr_t>(real_side) % 8 == 0 && (lay.howmany == 1 || real_dist % 2 == 0);
+  }
+  cudaError_t run(const void* in, void* out, void* ws, cudaStream_t st) const override {
+    if (r2c ? !paired(in, lay.idist) : !paired(out, lay.odist)) return generic->run(in, out, ws, st);
+    float2* work = static_cast<float2*>(ws);
+    void* iws = static_cast<char*>(ws) + work_bytes();
+    RealHalfLaunch L{};
+    L.work = work;
+    L.m = m;
+    L.istride = lay.istride;
+    L.idist = lay.idist;
+    L.ostride = lay.ostride;
+    L.odist = lay.odist;
+    L.scale = scale;
+    L.wmode_in = wmode_in;
+    L.wmode_out = wmode_out;
+    L.tw = tw.as<float2>();
+    for (int64_t m0 = 0; m0 < lay.howmany; m0 += chunk) {
+      const int64_t cnt = std::min(chunk, lay.howmany - m0);
+      const Node& c2c = (cnt < chunk && inner_last) ? *inner_last : *inner;
+      cudaError_t e;
+      if (r2c) {
+        const float2* z = static_cast<const float2*>(in) + m0 * (lay.idist / 2);
+        L.out = static_cast<float2*>(out);
+        e = c2c.run(z, work, iws, st);
+        if (e == cudaSuccess) e = launch_real_half(true, L, m0, cnt, st);
+      } else {
+        L.in = static_cast<const float2*>(in);
+        e = launch_real_half(false, L, m0, cnt, st);
+        if (e == cudaSuccess) e = c2c.run(work, static_cast<float2*>(out) + m0 * (lay.odist / 2), iws, st);
+      }
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+  std::string describe() const override {
+    std::ostringstream o;
+    o << "(" << (r2c ? "r2c" : "c2r") << "-half n=" << n << " m=" << m << " chunk=" << chunk << " "
+      << inner->describe() << ")";
+    return o.str();
+  }
+};
+
 }  // namespace
+
+static std::unique_ptr<Node> make_realwrap_generic(int kind, int64_t n, const Layout& lay, double scale,
+                                                   std::string* why, int wmode_in, int wmode_out, bool fp64);
 
 std::unique_ptr<Node> make_realwrap_node(int kind, int64_t n, const Layout& lay, double scale, std::string* why,
                                          int wmode_in, int wmode_out, bool fp64) {
+  // FP32 R2C / C2R of even n with unit real stride: the half-length form
+  const bool half = (kind == RW_R2C || kind == RW_C2R) && !fp64 && n >= 4 && n % 2 == 0 &&
+                    (kind == RW_R2C ? lay.istride == 1 : lay.ostride == 1) &&
+                    (kind == RW_R2C ? lay.idist >= n : lay.odist >= n) &&
+                    (kind == RW_R2C ? wmode_in == AW_NONE : wmode_out == AW_NONE) &&
+                    !std::getenv("PLFFT_B200_NO_REAL_HALF");
+  if (!half) return make_realwrap_generic(kind, n, lay, scale, why, wmode_in, wmode_out, fp64);
+  auto node = std::make_unique<RealHalfNode>();
+  node->r2c = kind == RW_R2C;
+  node->n = n;
+  node->m = n / 2;
+  node->lay = lay;
+  node->scale = float(scale);
+  node->wmode_in = wmode_in;
+  node->wmode_out = wmode_out;
+  node->generic = make_realwrap_generic(kind, n, lay, scale, why, wmode_in, wmode_out, false);
+  if (!node->generic) return nullptr;
+  const int64_t m = node->m;
+  const int64_t target = 64ll << 20;  // bytes of complex work per chunk
+  node->chunk = std::max<int64_t>(1, std::min<int64_t>(lay.howmany, target / (m * int64_t(sizeof(float2)))));
+  auto inner_for = [&](int64_t count) {
+    // R2C: pairs of the input (complex distance idist / 2) into work; C2R:
+    // work into pairs of the output (odist / 2), with the plan's scale
+    return node->r2c ? make_c2c_node(m, Layout{count, 1, lay.idist / 2, 1, m}, -1, 1.0f, 0, why)
+                     : make_c2c_node(m, Layout{count, 1, m, 1, lay.odist / 2}, +1, float(scale), 0, why);
+  };
+  node->inner = inner_for(node->chunk);
+  if (!node->inner) return nullptr;
+  const int64_t rem = lay.howmany % node->chunk;
+  if (rem) {
+    node->inner_last = inner_for(rem);
+    if (!node->inner_last) return nullptr;
+  }
+  std::vector<float2> tw(size_t(m) + 1);
+  for (int64_t k = 0; k <= m; ++k) {  // W_n^k
+    double c, sn;
+    unit_root(k, n, c, sn);
+    tw[k] = make_float2(float(c), float(-sn));
+  }
+  if (node->tw.upload(tw) != cudaSuccess) {
+    if (why) *why = "device allocation failed";
+    return nullptr;
+  }
+  return node;
+}
+
+static std::unique_ptr<Node> make_realwrap_generic(int kind, int64_t n, const Layout& lay, double scale,
+                                                   std::string* why, int wmode_in, int wmode_out, bool fp64) {
   if (kind == RW_DCT1 && n < 2) {
     if (why) *why = "DCT-I needs n > 1";
     return nullptr;

@@ -243,6 +243,71 @@ static cudaError_t launch_realwrap_t(bool pre, int kind, const RealWrapLaunch& L
   return cudaErrorInvalidValue;
 }
 
+// Half-length R2C / C2R for even n = 2m (FP32): the n reals of a member are
+// read as m complex pairs z_j = x_{2j} + i x_{2j+1}, so the complex DFT has
+// length m instead of n (the split / merge of the reference's R2C / C2R
+// twiddle levels, src/level_ab_t_r2c.cpp:17-120, src/level_ab_t_c2r.cpp:
+// 17-99).  With W = W_n^k and Z_m = Z_0:
+//   R2C, after Z = DFT_m(z):  X_k = E_k - i W O_k,  k = 0..m,
+//        E_k = (Z_k + conj Z_{m-k}) / 2,  O_k = (Z_k - conj Z_{m-k}) / 2;
+//   C2R, before z = IDFT_m(Z'):  Z'_k = (X_k + conj X_{m-k}) +
+//        i conj(W) (X_k - conj X_{m-k}),  k < m  (Im X_0, Im X_m ignored),
+//        then x_{2j} = Re z_j, x_{2j+1} = Im z_j.
+// The C2C of length m reads the R2C input (writes the C2R output) in place
+// of the user's buffer; these kernels are the split after it and the merge
+// before it.
+__global__ void __launch_bounds__(256) rhalf_r2c_post(const RealHalfLaunch L, int64_t m0, int64_t cnt) {
+  const int64_t m = L.m;
+  const int64_t total = cnt * (m + 1);
+  for (int64_t f = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; f < total; f += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t bl = f / (m + 1);
+    const int64_t k = f - bl * (m + 1);
+    const float2* Z = L.work + bl * m;
+    const float2 zk = Z[k == m ? 0 : k];
+    const float2 zm = Z[k == 0 ? 0 : m - k];
+    const float2 cm = make_float2(zm.x, -zm.y);
+    const float2 e = cscale(cadd(zk, cm), 0.5f);
+    const float2 o = cscale(csub(zk, cm), 0.5f);
+    const float2 wo = cmul(__ldg(L.tw + k), o);
+    const float sw = L.wmode_out ? L.scale * adj_weight(L.wmode_out, k, 2 * m) : L.scale;
+    L.out[(m0 + bl) * L.odist + k * L.ostride] = make_float2((e.x + wo.y) * sw, (e.y - wo.x) * sw);
+  }
+}
+
+__global__ void __launch_bounds__(256) rhalf_c2r_pre(const RealHalfLaunch L, int64_t m0, int64_t cnt) {
+  const int64_t m = L.m;
+  const int64_t total = cnt * m;
+  for (int64_t f = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; f < total; f += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t bl = f / m;
+    const int64_t k = f - bl * m;
+    const float2* X = L.in + (m0 + bl) * L.idist;
+    float2 xk = X[k * L.istride], xm = X[(m - k) * L.istride];
+    if (L.wmode_in) {
+      xk = cscale(xk, adj_weight(L.wmode_in, k, 2 * m));
+      xm = cscale(xm, adj_weight(L.wmode_in, m - k, 2 * m));
+    }
+    if (k == 0) {  // Im X_0 and Im X_m are ignored
+      xk.y = 0.f;
+      xm.y = 0.f;
+    }
+    const float2 cm = make_float2(xm.x, -xm.y);
+    const float2 a = cadd(xk, cm);
+    const float2 d = csub(xk, cm);
+    const float2 wd = cmulc(d, __ldg(L.tw + k));  // conj(W_n^k) d
+    L.work[bl * m + k] = cadd(a, make_float2(-wd.y, wd.x));
+  }
+}
+
+cudaError_t launch_real_half(bool r2c, const RealHalfLaunch& L, int64_t m0, int64_t cnt, cudaStream_t st) {
+  const int64_t total = cnt * (r2c ? L.m + 1 : L.m);
+  const unsigned blocks = unsigned(std::max<int64_t>(std::min<int64_t>((total + 255) / 256, 148 * 16), 1));
+  if (r2c)
+    rhalf_r2c_post<<<blocks, 256, 0, st>>>(L, m0, cnt);
+  else
+    rhalf_c2r_pre<<<blocks, 256, 0, st>>>(L, m0, cnt);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_realwrap(bool pre, int kind, const RealWrapLaunch& L, int64_t m0, int64_t cnt, cudaStream_t st) {
   return L.fp64 ? launch_realwrap_t<double>(pre, kind, L, m0, cnt, st)
                 : launch_realwrap_t<float>(pre, kind, L, m0, cnt, st);

@@ -225,3 +225,60 @@ def test_fused_r2c_in_place(n):
     plan.execute(d.data_ptr(), d.data_ptr())
     y = d.cpu().numpy().view(np.complex64).reshape(hm, h)
     assert oracle.rel_l2(y, oracle.r2c(xs.astype(np.float64))) <= oracle.fp32_tol(n)
+
+
+# half-length R2C / C2R (even n that is not twice a power of two): a length
+# n/2 C2C over the real data read as complex pairs, with the split / merge
+# kernel; odd real distances fall back to the full-length form.  Cases:
+# smooth, Rader and Bluestein half lengths, a four-step half length over two
+# chunks of members (the second one partial), strided complex sides.
+HALF_CASES = [(6, 7, 6, 4, 1), (10, 5, 10, 6, 1), (100, 33, 100, 51, 1), (1000, 64, 1000, 501, 1),
+              (2002, 9, 2002, 1002, 1), (2018, 6, 2018, 1010, 1), (2062, 6, 2062, 1032, 1),
+              (1000, 5, 1001, 501, 1), (1000, 4, 1000, 1100, 2), (100000, 200, 100000, 50001, 1)]
+
+
+@pytest.mark.parametrize("n,hm,rdist,cdist,cstride", HALF_CASES)
+def test_real_half(n, hm, rdist, cdist, cstride):
+    import torch
+
+    h = n // 2 + 1
+    rng = np.random.default_rng(n + hm)
+    rows = np.unique(np.array([0, hm // 2, hm - 1]))
+    x = rng.uniform(-1, 1, span(hm, rdist, n, 1)).astype(np.float32)
+    f = plfft.make_plan("r2c", n, hm, 1, rdist, cstride, cdist)
+    half = "half" in f.describe()
+    assert half, f.describe()
+    y = run_plan(f, x, span(hm, cdist, h, cstride), torch.complex64)
+    got = gather(y, hm, cdist, h, cstride)[rows]
+    ref = oracle.r2c(gather(x, hm, rdist, n, 1)[rows].astype(np.float64))
+    assert oracle.rel_l2(got, ref) <= oracle.fp32_tol(n), f.describe()
+    X = (rng.uniform(-1, 1, span(hm, cdist, h, cstride)) + 1j * rng.uniform(-1, 1, span(hm, cdist, h, cstride)))
+    X = X.astype(np.complex64)
+    b = plfft.make_plan("c2r", n, hm, cstride, cdist, 1, rdist, scale=1.0 / n)
+    assert "half" in b.describe(), b.describe()
+    z = run_plan(b, X, span(hm, rdist, n, 1), torch.float32)
+    refz = oracle.c2r(gather(X, hm, cdist, h, cstride)[rows].astype(np.complex128), n) / n
+    assert oracle.rel_l2(gather(z, hm, rdist, n, 1)[rows], refz) <= oracle.fp32_tol(n), b.describe()
+
+
+@pytest.mark.parametrize("n", [1000, 2018])
+def test_real_half_in_place(n):
+    """In-place R2C then C2R over the padded layout (each member's complex
+    output over its own real input)."""
+    import torch
+
+    hm = 7
+    h = n // 2 + 1
+    rng = np.random.default_rng(n)
+    x = np.zeros((hm, 2 * h), np.float32)
+    x[:, :n] = rng.uniform(-1, 1, (hm, n))
+    d = torch.from_numpy(x.ravel().copy()).cuda()
+    f = plfft.make_plan("r2c", n, hm, 1, 2 * h, 1, h, alias=plfft.IoAlias.MAY_ALIAS)
+    assert "half" in f.describe(), f.describe()
+    f.execute(d.data_ptr(), d.data_ptr())
+    Y = d.cpu().numpy().view(np.complex64).reshape(hm, h)
+    assert oracle.rel_l2(Y, oracle.r2c(x[:, :n].astype(np.float64))) <= oracle.fp32_tol(n)
+    b = plfft.make_plan("c2r", n, hm, 1, h, 1, 2 * h, alias=plfft.IoAlias.MAY_ALIAS, scale=1.0 / n)
+    b.execute(d.data_ptr(), d.data_ptr())
+    z = d.cpu().numpy().reshape(hm, 2 * h)[:, :n]
+    assert oracle.rel_l2(z, x[:, :n].astype(np.float64)) <= oracle.fp32_tol(n)
