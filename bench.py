@@ -714,8 +714,8 @@ def make_workload(name):
                                                 "c2c", 1009, 8192, profile="conv_rader_n1009_b8192"),
         "c2c_n1031_b8192": lambda: PlanWorkload("c2c_n1031_b8192", "C2C FP32 N=1031 (Bluestein) batch=8192",
                                                 "c2c", 1031, 8192, profile="conv_bluestein_n1031_b8192"),
-        "r2c_n1000_b16384": lambda: PlanWorkload("r2c_n1000_b16384", "R2C FP32 N=1000 (real wrap) batch=16384",
-                                                 "r2c", 1000, 16384, profile="realwrap_r2c_n1000_b16384"),
+        "r2c_n1000_b16384": lambda: PlanWorkload("r2c_n1000_b16384", "R2C FP32 N=1000 (half length) batch=16384",
+                                                 "r2c", 1000, 16384, profile="real_half_r2c_n1000_b16384"),
     }
     return table[name]()
 

@@ -256,13 +256,15 @@ static cudaError_t launch_realwrap_t(bool pre, int kind, const RealWrapLaunch& L
 // The C2C of length m reads the R2C input (writes the C2R output) in place
 // of the user's buffer; these kernels are the split after it and the merge
 // before it.
+// (a chunk holds at most 2^23 + chunk complex values, so element indices
+// within it fit 32 bits: 32-bit division instead of 64-bit)
 __global__ void __launch_bounds__(256) rhalf_r2c_post(const RealHalfLaunch L, int64_t m0, int64_t cnt) {
-  const int64_t m = L.m;
-  const int64_t total = cnt * (m + 1);
-  for (int64_t f = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; f < total; f += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t bl = f / (m + 1);
-    const int64_t k = f - bl * (m + 1);
-    const float2* Z = L.work + bl * m;
+  const uint32_t m = uint32_t(L.m);
+  const uint32_t total = uint32_t(cnt) * (m + 1);
+  for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < total; f += gridDim.x * blockDim.x) {
+    const uint32_t bl = f / (m + 1);
+    const uint32_t k = f - bl * (m + 1);
+    const float2* Z = L.work + size_t(bl) * m;
     const float2 zk = Z[k == m ? 0 : k];
     const float2 zm = Z[k == 0 ? 0 : m - k];
     const float2 cm = make_float2(zm.x, -zm.y);
@@ -270,18 +272,18 @@ __global__ void __launch_bounds__(256) rhalf_r2c_post(const RealHalfLaunch L, in
     const float2 o = cscale(csub(zk, cm), 0.5f);
     const float2 wo = cmul(__ldg(L.tw + k), o);
     const float sw = L.wmode_out ? L.scale * adj_weight(L.wmode_out, k, 2 * m) : L.scale;
-    L.out[(m0 + bl) * L.odist + k * L.ostride] = make_float2((e.x + wo.y) * sw, (e.y - wo.x) * sw);
+    L.out[(m0 + bl) * L.odist + int64_t(k) * L.ostride] = make_float2((e.x + wo.y) * sw, (e.y - wo.x) * sw);
   }
 }
 
 __global__ void __launch_bounds__(256) rhalf_c2r_pre(const RealHalfLaunch L, int64_t m0, int64_t cnt) {
-  const int64_t m = L.m;
-  const int64_t total = cnt * m;
-  for (int64_t f = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; f < total; f += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t bl = f / m;
-    const int64_t k = f - bl * m;
+  const uint32_t m = uint32_t(L.m);
+  const uint32_t total = uint32_t(cnt) * m;
+  for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < total; f += gridDim.x * blockDim.x) {
+    const uint32_t bl = f / m;
+    const uint32_t k = f - bl * m;
     const float2* X = L.in + (m0 + bl) * L.idist;
-    float2 xk = X[k * L.istride], xm = X[(m - k) * L.istride];
+    float2 xk = X[int64_t(k) * L.istride], xm = X[int64_t(m - k) * L.istride];
     if (L.wmode_in) {
       xk = cscale(xk, adj_weight(L.wmode_in, k, 2 * m));
       xm = cscale(xm, adj_weight(L.wmode_in, m - k, 2 * m));
@@ -294,7 +296,7 @@ __global__ void __launch_bounds__(256) rhalf_c2r_pre(const RealHalfLaunch L, int
     const float2 a = cadd(xk, cm);
     const float2 d = csub(xk, cm);
     const float2 wd = cmulc(d, __ldg(L.tw + k));  // conj(W_n^k) d
-    L.work[bl * m + k] = cadd(a, make_float2(-wd.y, wd.x));
+    L.work[size_t(bl) * m + k] = cadd(a, make_float2(-wd.y, wd.x));
   }
 }
 
