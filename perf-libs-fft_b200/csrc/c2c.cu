@@ -65,8 +65,11 @@ __device__ __forceinline__ float2 two_level(const TwoLevel& p, int e) {
 
 constexpr int kMaxTileC = 64;
 
+// two resident CTAs of the largest size: caps registers at 64 (16
+// elements per thread) or 128 (32) with no spills, so a typical 288-thread
+// tile fits three CTAs per SM instead of two
 template <int MAXE, int DIR>
-__global__ void __launch_bounds__(PLFFT_B200_TILE_THREADS(MAXE), 1) c2c_tile_kernel(const TileLaunch L) {
+__global__ void __launch_bounds__(PLFFT_B200_TILE_THREADS(MAXE), 2) c2c_tile_kernel(const TileLaunch L) {
   extern __shared__ float2 smem[];
   __shared__ int64_t ibase[kMaxTileC], obase[kMaxTileC];
   __shared__ int colidx[kMaxTileC];
