@@ -21,8 +21,9 @@ namespace plfft_b200 {
 __global__ void __launch_bounds__(256) bs_pre(const ConvLaunch L, int64_t m0, int64_t cnt) {
   const int64_t n = L.n, m = L.m;
   const int64_t total = cnt * m;
+  const bool small = total < (int64_t(1) << 31);
   for (int64_t f = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; f < total; f += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t bl = f / m;
+    const int64_t bl = flat_div(f, m, small);
     const int64_t j = f - bl * m;
     float2 z = make_float2(0.f, 0.f);
     if (j < n) z = cmul(L.in[(m0 + bl) * L.idist + j * L.istride], L.chirp[j]);
@@ -34,8 +35,9 @@ __global__ void __launch_bounds__(256) bs_pre(const ConvLaunch L, int64_t m0, in
 __global__ void __launch_bounds__(256) conv_mul(const ConvLaunch L, int64_t cnt, int save0) {
   const int64_t m = L.m;
   const int64_t total = cnt * m;
+  const bool small = total < (int64_t(1) << 31);
   for (int64_t f = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; f < total; f += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t bl = f / m;
+    const int64_t bl = flat_div(f, m, small);
     const int64_t k = f - bl * m;
     const float2 a = L.work[f];
     if (save0 && k == 0) L.sum0[bl] = a;
@@ -46,9 +48,10 @@ __global__ void __launch_bounds__(256) conv_mul(const ConvLaunch L, int64_t cnt,
 __global__ void __launch_bounds__(256) bs_post(const ConvLaunch L, int64_t m0, int64_t cnt) {
   const int64_t n = L.n, m = L.m;
   const int64_t total = cnt * n;
+  const bool small = total < (int64_t(1) << 31);
   const float s = L.scale;
   for (int64_t f = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; f < total; f += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t bl = f / n;
+    const int64_t bl = flat_div(f, n, small);
     const int64_t k = f - bl * n;
     const float2 y = cmul(L.work[bl * m + k], L.chirp[k]);
     L.out[(m0 + bl) * L.odist + k * L.ostride] = cscale(y, s);
@@ -58,8 +61,9 @@ __global__ void __launch_bounds__(256) bs_post(const ConvLaunch L, int64_t m0, i
 __global__ void __launch_bounds__(256) rd_pre(const ConvLaunch L, int64_t m0, int64_t cnt) {
   const int64_t m = L.m;  // P - 1
   const int64_t total = cnt * m;
+  const bool small = total < (int64_t(1) << 31);
   for (int64_t f = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; f < total; f += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t bl = f / m;
+    const int64_t bl = flat_div(f, m, small);
     const int64_t q = f - bl * m;
     L.work[f] = L.in[(m0 + bl) * L.idist + int64_t(L.perm_in[q]) * L.istride];
   }
@@ -68,9 +72,10 @@ __global__ void __launch_bounds__(256) rd_pre(const ConvLaunch L, int64_t m0, in
 __global__ void __launch_bounds__(256) rd_post(const ConvLaunch L, int64_t m0, int64_t cnt) {
   const int64_t m = L.m;
   const int64_t total = cnt * m;
+  const bool small = total < (int64_t(1) << 31);
   const float s = L.scale;
   for (int64_t f = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; f < total; f += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t bl = f / m;
+    const int64_t bl = flat_div(f, m, small);
     const int64_t q = f - bl * m;
     const int64_t b = m0 + bl;
     const float2 x0 = L.in[b * L.idist];

@@ -95,9 +95,10 @@ __global__ void __launch_bounds__(256) realwrap_pre(const RealWrapLaunch L, int6
   using C = typename CplxOf<R>::type;
   const int64_t n = L.n, len = L.len;
   const int64_t total = cnt * len;
+  const bool small = total < (int64_t(1) << 31);
   C* work = static_cast<C*>(L.work);
   for (int64_t f = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; f < total; f += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t bl = f / len;
+    const int64_t bl = flat_div(f, len, small);
     const int64_t j = f - bl * len;
     const int64_t b = m0 + bl;
     C z = cx<R>(0, 0);
@@ -163,9 +164,10 @@ __global__ void __launch_bounds__(256) realwrap_post(const RealWrapLaunch L, int
   using C = typename CplxOf<R>::type;
   const int64_t n = L.n, len = L.len, nout = L.nout;
   const int64_t total = cnt * nout;
+  const bool small = total < (int64_t(1) << 31);
   const R s = R(L.scale);
   for (int64_t f = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; f < total; f += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t bl = f / nout;
+    const int64_t bl = flat_div(f, nout, small);
     const int64_t k = f - bl * nout;
     const int64_t b = m0 + bl;
     const C* F = static_cast<const C*>(L.work) + bl * len;

@@ -29,6 +29,13 @@
 
 namespace plfft_b200 {
 
+// f / d for the flat element loops of the elementwise kernels: 32-bit
+// division (a short sequence) when the loop's range fits 31 bits, which the
+// 64 MB chunks of those kernels guarantee in practice
+__device__ __forceinline__ int64_t flat_div(int64_t f, int64_t d, bool small) {
+  return small ? int64_t(uint32_t(f) / uint32_t(d)) : f / d;
+}
+
 // shared-memory index padding: one spare complex every 16 (128 bytes)
 __device__ __forceinline__ int spad(int p) { return p + (p >> 4); }
 
