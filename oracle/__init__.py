@@ -146,6 +146,9 @@ def _libq():
         for name in ("oracle_q15_c2c", "oracle_q7_c2c"):
             getattr(L, name).argtypes = [dp, dp, i64, i64, i64, i64, ctypes.c_int]
             getattr(L, name).restype = ctypes.c_int
+        for name in ("oracle_q15_r2c", "oracle_q7_r2c"):
+            getattr(L, name).argtypes = [dp, dp, i64, i64, i64, i64, i64, i64]
+            getattr(L, name).restype = ctypes.c_int
         L.oracle_q15_twiddles.argtypes = [i64, ctypes.c_int, dp]
         L.oracle_q15_twiddles.restype = None
         _LIBQ = L
@@ -170,6 +173,49 @@ def q15_c2c(x, direction=-1):
 def q7_c2c(x, direction=-1):
     """x: int8 [howmany, n, 2] (re, im) -> int8 [howmany, n, 2], scaled by 1/n."""
     return _fixed_c2c(x, direction, np.int8, _libq().oracle_q7_c2c)
+
+
+def _fixed_r2c(x, dtype, fn, odist_unit):
+    x = np.ascontiguousarray(x, dtype=dtype)
+    hm, n = x.shape[0], x.shape[1]
+    h = n // 2 + 1
+    if odist_unit and hm > 1:
+        # members adjacent in the output (ostride hm, odist 1): the reference's
+        # uu / gu kernel variants for n <= 16
+        y = np.empty((h, hm, 2), dtype)
+        rc = fn(_ptr(x), _ptr(y), n, hm, 1, n, hm, 1)
+        y = np.ascontiguousarray(y.transpose(1, 0, 2))
+    else:
+        y = np.empty((hm, h, 2), dtype)
+        rc = fn(_ptr(x), _ptr(y), n, hm, 1, n, 1, h)
+    if rc != 0:
+        raise ValueError(f"fixed-point oracle: unsupported length {n}")
+    return y
+
+
+def fixed_r2c_strided(bits, buf, n, howmany, istride, idist, ostride, odist, out_elems):
+    """R2C of the members of the flat real buffer buf (int16 for bits 16, int8
+    for 8) in the given layout; returns a flat complex buffer [out_elems, 2]
+    (zero where no output lands)."""
+    dtype = np.int16 if bits == 16 else np.int8
+    buf = np.ascontiguousarray(buf, dtype=dtype)
+    y = np.zeros((out_elems, 2), dtype)
+    fn = _libq().oracle_q15_r2c if bits == 16 else _libq().oracle_q7_r2c
+    if fn(_ptr(buf), _ptr(y), n, howmany, istride, idist, ostride, odist) != 0:
+        raise ValueError(f"fixed-point oracle: unsupported length {n}")
+    return y
+
+
+def q15_r2c(x, odist_unit=False):
+    """x: int16 [howmany, n] reals -> int16 [howmany, n/2+1, 2], scaled by 1/n.
+    odist_unit: compute as a batch laid out with output distance 1."""
+    return _fixed_r2c(x, np.int16, _libq().oracle_q15_r2c, odist_unit)
+
+
+def q7_r2c(x, odist_unit=False):
+    """x: int8 [howmany, n] reals -> int8 [howmany, n/2+1, 2], scaled by 1/n.
+    odist_unit: compute as a batch laid out with output distance 1."""
+    return _fixed_r2c(x, np.int8, _libq().oracle_q7_r2c, odist_unit)
 
 
 def q15_twiddles(n, direction=-1):

@@ -364,6 +364,197 @@ static int fixed_c2c(int bits, const void *in, void *out, int64_t n, int64_t how
   return 0;
 }
 
+/* The reference's 8-point real-input codelet (plfft_8_*_hjjnfoh, forward):
+ * with a_k = x_k pre-shifted by 3, d/s = saturating differences / sums,
+ *   g = d15 - d37, h = d15 + d37, e1 = s15 - s37, f1 = s15 + s37,
+ *   p = s04 - s26, q = s04 + s26,
+ *   X0 = (q + f1, 0), X4 = (q - f1, 0), X2 = (rdm(p, 1), rdm(e1, -1)),
+ *   X1 = (rdm(d04 + rdm(g, c8), 1), rdm(d26 + rdm(h, c8), -1)),
+ *   X3 = (d04 - rdm(g, c8), d26 - rdm(h, c8)),
+ * where 1 and -1 are the format's 1 - 2^-(B-1) and -1 (the uun, us and gs
+ * variants).  Bins 1 and 3 round differently from the complex codelet on
+ * (x, 0); bins 5..7 are not used. */
+static void real8(const fmt *f, const int32_t *x, fc *y) {
+  int32_t a[8];
+  for (int k = 0; k < 8; ++k) a[k] = rshr(x[k], 3);
+  const int32_t d15 = sat(f, a[1] - a[5]), s15 = sat(f, a[1] + a[5]);
+  const int32_t d26 = sat(f, a[2] - a[6]), s26 = sat(f, a[2] + a[6]);
+  const int32_t d37 = sat(f, a[3] - a[7]), s37 = sat(f, a[3] + a[7]);
+  const int32_t d04 = sat(f, a[0] - a[4]), s04 = sat(f, a[0] + a[4]);
+  const int32_t e1 = sat(f, s15 - s37), f1 = sat(f, s15 + s37);
+  const int32_t g = sat(f, d15 - d37), h = sat(f, d15 + d37);
+  const int32_t rg = rdm(f, g, f->c8), rh = rdm(f, h, f->c8);
+  const int32_t p = sat(f, s04 - s26), q = sat(f, s04 + s26);
+  y[0] = (fc){sat(f, q + f1), 0};
+  y[4] = (fc){sat(f, q - f1), 0};
+  y[2] = (fc){rdm(f, p, f->one), rdm(f, e1, f->mone)};
+  y[1] = (fc){rdm(f, sat(f, d04 + rg), f->one), rdm(f, sat(f, d26 + rh), f->mone)};
+  y[3] = (fc){sat(f, d04 - rg), sat(f, d26 - rh)};
+  for (int k = 5; k < 8; ++k) y[k] = (fc){0, 0};
+}
+
+/* The reference's 8-point real-input codelet in its unit-output-distance
+ * batch variant (plfft_8_*_hjjnfoh_uu / _gu, which also runs as the first
+ * stage of every larger R2C plan, vectorised across its columns): the same
+ * sums as real8, with
+ *   X2 = (p, -rdm(e1, 1)), X1 = (d04 + rdm(g, c8), -rdm(d26 + rdm(h, c8), 1)),
+ *   X3 = (d04 - rdm(g, c8), rdm(d26 - rdm(h, c8), 1))
+ * (negations saturating). */
+static void real8_uo(const fmt *f, const int32_t *x, fc *y) {
+  int32_t a[8];
+  for (int k = 0; k < 8; ++k) a[k] = rshr(x[k], 3);
+  const int32_t d15 = sat(f, a[1] - a[5]), s15 = sat(f, a[1] + a[5]);
+  const int32_t d26 = sat(f, a[2] - a[6]), s26 = sat(f, a[2] + a[6]);
+  const int32_t d37 = sat(f, a[3] - a[7]), s37 = sat(f, a[3] + a[7]);
+  const int32_t d04 = sat(f, a[0] - a[4]), s04 = sat(f, a[0] + a[4]);
+  const int32_t e1 = sat(f, s15 - s37), f1 = sat(f, s15 + s37);
+  const int32_t g = sat(f, d15 - d37), h = sat(f, d15 + d37);
+  const int32_t rg = rdm(f, g, f->c8), rh = rdm(f, h, f->c8);
+  const int32_t p = sat(f, s04 - s26), q = sat(f, s04 + s26);
+  y[0] = (fc){sat(f, q + f1), 0};
+  y[4] = (fc){sat(f, q - f1), 0};
+  y[2] = (fc){p, sat(f, -(int64_t)rdm(f, e1, f->one))};
+  y[1] = (fc){sat(f, d04 + rg), sat(f, -(int64_t)rdm(f, sat(f, d26 + rh), f->one))};
+  y[3] = (fc){sat(f, d04 - rg), rdm(f, sat(f, d26 - rh), f->one)};
+  for (int k = 5; k < 8; ++k) y[k] = (fc){0, 0};
+}
+
+/* The 4-point real-input codelet of the single-member and strided-output
+ * variants (plfft_4_*_hjjnfoh / rppnfoh, uun, us, gs): X0, X2 as the complex
+ * codelet, X1 = (rdm(a0 - a2, 1), rdm(a1 - a3, -1)).  The unit-output-distance
+ * variants (uu, gu) compute X1 as the complex codelet does. */
+static void real4(const fmt *f, const int32_t *x, fc *y) {
+  int32_t a[4];
+  for (int k = 0; k < 4; ++k) a[k] = rshr(x[k], 2);
+  const int32_t s02 = sat(f, a[0] + a[2]), d02 = sat(f, a[0] - a[2]);
+  const int32_t s13 = sat(f, a[1] + a[3]), d13 = sat(f, a[1] - a[3]);
+  y[0] = (fc){sat(f, s02 + s13), 0};
+  y[2] = (fc){sat(f, s02 - s13), 0};
+  y[1] = (fc){rdm(f, d02, f->one), rdm(f, d13, f->mone)};
+  y[3] = (fc){0, 0};
+}
+
+/* real-input codelet of length r <= 16 on x.  uo selects the
+ * unit-output-distance kernel variant (uu, gu: a batch whose members are
+ * adjacent in the output), which is also the first stage of the larger
+ * plans; the others (uun, us, gs) use real8 and real4.  Lengths 2 and 16, and
+ * length 4 of the uo variants, are the complex codelet on (x, 0). */
+static void real_codelet(const fmt *f, int r, int uo, const int32_t *x, fc *y) {
+  if (r == 8) {
+    if (uo)
+      real8_uo(f, x, y);
+    else
+      real8(f, x, y);
+    return;
+  }
+  if (r == 4 && !uo) {
+    real4(f, x, y);
+    return;
+  }
+  const int s = ilog2(r);
+  fc a[16];
+  for (int k = 0; k < r; ++k) a[k] = (fc){rshr(x[k], s), 0};
+  codelet(f, r, -1, a, y);
+}
+
+/* fixed-point R2C (forward) of power-of-two n in [2, 4096]: the reference's
+ * R2C plans run the same levels as the C2C ones on the real input (imaginary
+ * parts zero), but each twiddled radix-16 level computes only the rows
+ * r <= rows/2 of its sub-spectra and writes row rows - r (r >= 1) as the
+ * conjugate of row r with the codelet outputs reversed: output k of row
+ * rows - r is conj(output 15 - k of row r), from X[L - b] = conj(X[b]) for
+ * the length-L sub-spectrum of a real sequence (the R2C twiddled levels
+ * with conjugate-reversed second output,
+ * planner/strategies/cooley_tukey.hpp:145-248, 386-470, and the kernels
+ * plfft_ab / ac _q15_jjjtfj_dit).  The length-n/16 and n/256 first-stage
+ * codelets read only bins <= half their length: the reference's real-input
+ * kernels in their uu variant (real_codelet with uo set).  A plan of n <= 16
+ * is one real-input kernel whose variant follows the batch layout
+ * (providers/aot/aot_kernel_data.cpp:188-252): uu or gu when the batch has
+ * more than one member and odist is 1, else uun, us or gs.  Outputs: bins
+ * 0..n/2, ostride complex elements apart, members odist apart; inputs
+ * istride reals apart, members idist apart. */
+static int fixed_r2c(int bits, const void *in, void *out, int64_t n, int64_t howmany, int64_t istride,
+                     int64_t idist, int64_t ostride, int64_t odist) {
+  if (n < 2 || n > 4096 || (n & (n - 1))) return -1;
+  const fmt F = make_fmt(bits), *f = &F;
+  const size_t esz = (size_t)(bits / 4), rsz = (size_t)(bits / 8);
+  const int64_t h = n / 2 + 1;
+  fc *x = (fc *)malloc(sizeof(fc) * (size_t)n);
+  fc *y = (fc *)malloc(sizeof(fc) * (size_t)n);
+  int32_t *w = NULL, *w2 = NULL;
+  fc *b1 = NULL, *b0 = NULL;
+  const int64_t m = n / 16, m2 = n > 256 ? n / 256 : 0, first = n > 256 ? m2 : m, cols = n > 16 ? n / first : 0;
+  if (n > 16) {
+    w = (int32_t *)malloc(sizeof(int32_t) * 4 * 15 * (size_t)(m > 1 ? m - 1 : 1));
+    w2 = (int32_t *)malloc(sizeof(int32_t) * 4 * 15 * (size_t)(m2 > 1 ? m2 - 1 : 1));
+    b1 = (fc *)malloc(sizeof(fc) * (size_t)n);
+    b0 = (fc *)malloc(sizeof(fc) * (size_t)n);
+    twiddles16(f, m, -1, w);
+    if (m2) twiddles16(f, m2, -1, w2);
+  }
+  for (int64_t b = 0; b < howmany; ++b) {
+    for (int64_t k = 0; k < n; ++k) {
+      const char *p = (const char *)in + rsz * (size_t)(b * idist + k * istride);
+      x[k] = (fc){bits == 16 ? *(const int16_t *)p : *(const int8_t *)p, 0};
+    }
+    if (n <= 16) {
+      int32_t r[16];
+      for (int k = 0; k < n; ++k) r[k] = x[k].re;
+      real_codelet(f, (int)n, howmany > 1 && odist == 1, r, y);
+    } else {
+      for (int64_t c = 0; c < cols; ++c) {
+        int32_t r[16];
+        fc yy[16];
+        for (int q = 0; q < first; ++q) r[q] = x[c + cols * q].re;
+        real_codelet(f, (int)first, 1, r, yy);
+        for (int k = 0; k < first; ++k) b1[c + cols * k] = yy[k];
+      }
+      const fc *rows = b1;
+      if (m2) { /* inner radix-16 level: rows i0 > m2/2 mirrored */
+        for (int64_t i0 = 0; i0 <= m2 / 2; ++i0)
+          for (int t = 0; t < 16; ++t) {
+            fc v[16], yy[16];
+            for (int i = 0; i < 16; ++i) v[i] = b1[256 * i0 + t + 16 * i];
+            twiddled16(f, -1, v, i0, w2, yy);
+            for (int k = 0; k < 16; ++k) {
+              b0[16 * i0 + t + 16 * m2 * k] = yy[k];
+              if (i0 > 0 && 2 * i0 < m2)
+                b0[16 * (m2 - i0) + t + 16 * m2 * (15 - k)] = (fc){yy[k].re, -yy[k].im};
+            }
+          }
+        rows = b0;
+      }
+      for (int64_t j = 0; j <= m / 2; ++j) { /* outer radix-16 level: rows j > m/2 mirrored */
+        fc yy[16];
+        twiddled16(f, -1, rows + 16 * j, j, w, yy);
+        for (int k = 0; k < 16; ++k) {
+          y[j + m * k] = yy[k];
+          if (j > 0 && 2 * j < m) y[(m - j) + m * (15 - k)] = (fc){yy[k].re, -yy[k].im};
+        }
+      }
+    }
+    for (int64_t k = 0; k < h; ++k) st(bits, (char *)out + esz * (size_t)(b * odist + k * ostride), 0, y[k]);
+  }
+  free(x);
+  free(y);
+  free(w);
+  free(w2);
+  free(b1);
+  free(b0);
+  return 0;
+}
+
+int oracle_q15_r2c(const int16_t *in, int16_t *out, int64_t n, int64_t howmany, int64_t istride, int64_t idist,
+                   int64_t ostride, int64_t odist) {
+  return fixed_r2c(16, in, out, n, howmany, istride, idist, ostride, odist);
+}
+
+int oracle_q7_r2c(const int8_t *in, int8_t *out, int64_t n, int64_t howmany, int64_t istride, int64_t idist,
+                  int64_t ostride, int64_t odist) {
+  return fixed_r2c(8, in, out, n, howmany, istride, idist, ostride, odist);
+}
+
 int oracle_q15_c2c(const int16_t *in, int16_t *out, int64_t n, int64_t howmany, int64_t idist, int64_t odist,
                    int dir) {
   return fixed_c2c(16, in, out, n, howmany, idist, odist, dir);

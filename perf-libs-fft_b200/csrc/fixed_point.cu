@@ -45,6 +45,8 @@
 // inner level per thread, one outer row per thread.
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "kernels.h"
 #include "launch_pdl.cuh"
 #include "ptx.cuh"
@@ -384,6 +386,245 @@ __global__ void __launch_bounds__(256) fx_three_stage_kernel(const FixedLaunch L
   }
 }
 
+// ---- R2C (forward): the reference's real-input plans ----
+// The reference's R2C plans run the C2C levels on the real input (imaginary
+// parts zero) but each twiddled radix-16 level computes only the rows
+// r <= rows/2 of its sub-spectra and writes row rows - r (r >= 1) as the
+// conjugate of row r with the codelet outputs reversed (output k of row
+// rows - r = conj(output 15 - k of row r): X[L - b] = conj(X[b]) for the
+// length-L sub-spectrum of a real sequence; planner/strategies/
+// cooley_tukey.hpp:145-248, 386-470).  The real-input codelets come in
+// kernel variants that round differently at lengths 4 and 8
+// (providers/aot/aot_kernel_data.cpp:188-252): the unit-output-distance ones
+// (uu, gu: a batch of more than one member with odist 1, and the first stage
+// of every larger plan) and the others (uun, us, gs).  Lengths 2 and 16,
+// and length 4 of the unit-output-distance variants, are the complex codelet
+// on (x, 0).  Outputs are bins 0..n/2.
+
+// scalar storage of one real lane
+template <int B>
+using FxS = typename std::conditional<B == 16, short, signed char>::type;
+
+template <int B>
+__device__ __forceinline__ int fx_sat(int v) {
+  return max(Fx<B>::LO, min(Fx<B>::HI, v));
+}
+
+// the reference's 8-point real-input codelet (forward), on raw reals.
+// UO false (uun, us, gs): X2 = (rdm(p, 1), rdm(e1, -1)),
+//   X1 = (rdm(d04 + rg, 1), rdm(d26 + rh, -1)), X3 = (d04 - rg, d26 - rh);
+// UO true (uu, gu): X2 = (p, -rdm(e1, 1)),
+//   X1 = (d04 + rg, -rdm(d26 + rh, 1)), X3 = (d04 - rg, rdm(d26 - rh, 1));
+// rg, rh = rdm(g, c8), rdm(h, c8); 1 and -1 are the format's HI and LO.
+// Every intermediate is within range after the 3-bit pre-shift, so the
+// negations are exact.
+template <int B, bool UO>
+__device__ __forceinline__ void q_real8(const int* x, qc* y) {
+  using A = Ar<B>;
+  constexpr int C8 = Fx<B>::C8, HI = Fx<B>::HI, LO = Fx<B>::LO;
+  int a[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = rshr(x[k], 3);
+  const int d15 = fx_sat<B>(a[1] - a[5]), s15 = fx_sat<B>(a[1] + a[5]);
+  const int d26 = fx_sat<B>(a[2] - a[6]), s26 = fx_sat<B>(a[2] + a[6]);
+  const int d37 = fx_sat<B>(a[3] - a[7]), s37 = fx_sat<B>(a[3] + a[7]);
+  const int d04 = fx_sat<B>(a[0] - a[4]), s04 = fx_sat<B>(a[0] + a[4]);
+  const int e1 = fx_sat<B>(s15 - s37), f1 = fx_sat<B>(s15 + s37);
+  const int g = fx_sat<B>(d15 - d37), h = fx_sat<B>(d15 + d37);
+  const int rg = A::template rdm<C8>(g), rh = A::template rdm<C8>(h);
+  const int p = fx_sat<B>(s04 - s26), q = fx_sat<B>(s04 + s26);
+  y[0] = {fx_sat<B>(q + f1), 0};
+  y[4] = {fx_sat<B>(q - f1), 0};
+  if constexpr (UO) {
+    y[2] = {p, -A::template rdm<HI>(e1)};
+    y[1] = {fx_sat<B>(d04 + rg), -A::template rdm<HI>(fx_sat<B>(d26 + rh))};
+    y[3] = {fx_sat<B>(d04 - rg), A::template rdm<HI>(fx_sat<B>(d26 - rh))};
+  } else {
+    y[2] = {A::template rdm<HI>(p), A::template rdm<LO>(e1)};
+    y[1] = {A::template rdm<HI>(fx_sat<B>(d04 + rg)), A::template rdm<LO>(fx_sat<B>(d26 + rh))};
+    y[3] = {fx_sat<B>(d04 - rg), fx_sat<B>(d26 - rh)};
+  }
+  y[5] = y[6] = y[7] = {0, 0};
+}
+
+// the 4-point real-input codelet of the uun / us / gs variants: X0, X2 as
+// the complex codelet, X1 = (rdm(a0 - a2, 1), rdm(a1 - a3, -1))
+template <int B>
+__device__ __forceinline__ void q_real4(const int* x, qc* y) {
+  using A = Ar<B>;
+  int a[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) a[k] = rshr(x[k], 2);
+  const int s02 = a[0] + a[2], d02 = a[0] - a[2], s13 = a[1] + a[3], d13 = a[1] - a[3];
+  y[0] = {s02 + s13, 0};
+  y[2] = {s02 - s13, 0};
+  y[1] = {A::template rdm<Fx<B>::HI>(d02), A::template rdm<Fx<B>::LO>(d13)};
+  y[3] = {0, 0};
+}
+
+// real-input codelet of length R on raw reals; UO selects the
+// unit-output-distance variant
+template <int R, int B, bool UO>
+__device__ __forceinline__ void q_real_codelet(const int* x, qc* y) {
+  if constexpr (R == 8) {
+    q_real8<B, UO>(x, y);
+  } else if constexpr (R == 4 && !UO) {
+    q_real4<B>(x, y);
+  } else {
+    constexpr int S = ilog2_c(R);
+    qc a[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) a[k] = {S ? rshr(x[k], S) : x[k], 0};
+    q_dft<R, B>(a, y);
+  }
+}
+
+template <int B>
+__device__ __forceinline__ qc fx_conj(qc v) { return {v.re, -v.im}; }
+
+// n <= 16: one thread per member
+template <int N, int B, bool UO>
+__global__ void __launch_bounds__(256) fx_r2c_small_kernel(const FixedLaunch L) {
+  using W = typename Fx<B>::W;
+  griddep_wait();  // launched programmatically (launch_pdl.cuh)
+  griddep_launch_dependents();
+  const int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b >= L.howmany) return;
+  const FxS<B>* x = static_cast<const FxS<B>*>(L.in) + b * L.idist;
+  W* y = static_cast<W*>(L.out) + b * L.odist;
+  int xr[N];
+  qc r[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) xr[k] = x[k * L.istride];
+  q_real_codelet<N, B, UO>(xr, r);
+#pragma unroll
+  for (int k = 0; k <= N / 2; ++k) y[k * L.ostride] = pack<B>(r[k]);
+}
+
+// n = 16 m, m = 2..16: G = blockDim / 16 members per CTA; rows j <= m/2
+template <int N, int B>
+__global__ void __launch_bounds__(256) fx_r2c_two_stage_kernel(const FixedLaunch L) {
+  using W = typename Fx<B>::W;
+  griddep_wait();  // launched programmatically (launch_pdl.cuh)
+  griddep_launch_dependents();
+  constexpr int M = N / 16, PITCH = fx_pitch(N), ROWS = M / 2 + 1;
+  extern __shared__ __align__(16) unsigned char fsm[];
+  short4* tw = reinterpret_cast<short4*>(fsm);  // (c, s, cvt(-s), c)
+  W* tile = reinterpret_cast<W*>(tw + 15 * (M - 1 > 0 ? M - 1 : 1));
+  const int G = blockDim.x / 16;
+  const int64_t b0 = int64_t(blockIdx.x) * G;
+  const int64_t left = L.howmany - b0;
+  const int cnt = left < G ? int(left) : G;
+  for (int i = threadIdx.x; i < 15 * (M - 1); i += blockDim.x) tw[i] = L.tw[i];
+  const FxS<B>* in = static_cast<const FxS<B>*>(L.in);
+  for (int f = threadIdx.x; f < cnt * N; f += blockDim.x) {
+    const int g = f / N, k = f - g * N;
+    tile[g * PITCH + fx_pos(k)] = pack<B>(qc{in[(b0 + g) * L.idist + int64_t(k) * L.istride], 0});
+  }
+  __syncthreads();
+  const int g = threadIdx.x >> 4, c = threadIdx.x & 15;
+  W* mine = tile + g * PITCH;
+  if (g < cnt) {  // stage 1: length-M real codelet down column c, in place
+    int xr[M];
+    qc r[M];
+#pragma unroll
+    for (int q = 0; q < M; ++q) xr[q] = unpack(mine[fx_pos(c + 16 * q)]).re;
+    q_real_codelet<M, B, true>(xr, r);
+#pragma unroll
+    for (int k = 0; k < M; ++k) mine[fx_pos(c + 16 * k)] = pack<B>(r[k]);
+  }
+  __syncthreads();
+  // stage 2: rows (member, j <= M/2); row M - j is the mirror of row j
+  for (int row = threadIdx.x; row < cnt * ROWS; row += blockDim.x) {
+    const int gg = row / ROWS, j = row - gg * ROWS;
+    const W* src = tile + gg * PITCH + fx_pos(16 * j);
+    qc a[16], r[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const qc s = pre<B>(unpack(src[i]), 4);
+      a[i] = (i == 0 || j == 0) ? s : Ar<B>::twiddle(s, tw[15 * (j - 1) + (i - 1)]);
+    }
+    q_dft<16, B>(a, r);
+    W* y = static_cast<W*>(L.out) + (b0 + gg) * L.odist;
+    const bool mirror = j > 0 && 2 * j < M;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const int t = j + M * k, tm = (M - j) + M * (15 - k);
+      if (t <= N / 2) y[int64_t(t) * L.ostride] = pack<B>(r[k]);
+      if (mirror && tm <= N / 2) y[int64_t(tm) * L.ostride] = pack<B>(fx_conj<B>(r[k]));
+    }
+  }
+}
+
+// n = 256 m', m' = 2..16: one member per CTA of 256 threads
+template <int N, int B>
+__global__ void __launch_bounds__(256) fx_r2c_three_stage_kernel(const FixedLaunch L) {
+  using W = typename Fx<B>::W;
+  griddep_wait();  // launched programmatically (launch_pdl.cuh)
+  griddep_launch_dependents();
+  constexpr int M2 = N / 256, M = N / 16;
+  extern __shared__ __align__(16) unsigned char fsm[];
+  W* t = reinterpret_cast<W*>(fsm);
+  const int64_t b = blockIdx.x;
+  const FxS<B>* x = static_cast<const FxS<B>*>(L.in) + b * L.idist;
+  W* y = static_cast<W*>(L.out) + b * L.odist;
+  for (int k = threadIdx.x; k < N; k += 256) t[fx_pos(k)] = pack<B>(qc{x[int64_t(k) * L.istride], 0});
+  __syncthreads();
+  {  // length-M2 real codelet down column c = threadIdx.x, in place
+    const int c = threadIdx.x;
+    int xr[M2];
+    qc r[M2];
+#pragma unroll
+    for (int q = 0; q < M2; ++q) xr[q] = unpack(t[fx_pos(c + 256 * q)]).re;
+    q_real_codelet<M2, B, true>(xr, r);
+#pragma unroll
+    for (int k = 0; k < M2; ++k) t[fx_pos(c + 256 * k)] = pack<B>(r[k]);
+  }
+  __syncthreads();
+  // inner radix-16 level: task (row i0 <= M2/2, column tc); row M2 - i0 is
+  // the mirror of row i0
+  const int i0 = threadIdx.x >> 4, tc = threadIdx.x & 15;
+  const bool act = i0 <= M2 / 2;
+  qc r[16];
+  if (act) {
+    qc a[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const qc s = pre<B>(unpack(t[fx_pos(256 * i0 + tc + 16 * i)]), 4);
+      a[i] = (i == 0 || i0 == 0) ? s : Ar<B>::twiddle(s, __ldg(L.tw2 + 15 * (i0 - 1) + (i - 1)));
+    }
+    q_dft<16, B>(a, r);
+  }
+  __syncthreads();  // every input of this level is read before any output lands
+  if (act) {
+    const bool mirror = i0 > 0 && 2 * i0 < M2;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      t[fx_pos(16 * i0 + tc + 16 * M2 * k)] = pack<B>(r[k]);
+      if (mirror) t[fx_pos(16 * (M2 - i0) + tc + 16 * M2 * (15 - k))] = pack<B>(fx_conj<B>(r[k]));
+    }
+  }
+  __syncthreads();
+  // outer radix-16 level: rows j <= M/2, row M - j the mirror of row j
+  if (threadIdx.x <= M / 2) {
+    const int j = threadIdx.x;
+    qc a[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const qc s = pre<B>(unpack(t[fx_pos(16 * j + i)]), 4);
+      a[i] = (i == 0 || j == 0) ? s : Ar<B>::twiddle(s, __ldg(L.tw + 15 * (j - 1) + (i - 1)));
+    }
+    q_dft<16, B>(a, r);
+    const bool mirror = j > 0 && 2 * j < M;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const int tt = j + M * k, tm = (M - j) + M * (15 - k);
+      if (tt <= N / 2) y[int64_t(tt) * L.ostride] = pack<B>(r[k]);
+      if (mirror && tm <= N / 2) y[int64_t(tm) * L.ostride] = pack<B>(fx_conj<B>(r[k]));
+    }
+  }
+}
+
 bool fixed_supported(int64_t n) { return n >= 1 && n <= 4096 && (n & (n - 1)) == 0; }
 
 template <int B>
@@ -408,6 +649,48 @@ static cudaError_t run_fx(const FixedLaunch& L, cudaStream_t st) {
     const int smem = fx_smem_bytes<B>(N, 1);
     return launch_pdl(fx_three_stage_kernel<N, DIR, B>, dim3(unsigned(L.howmany)), dim3(256), size_t(smem), st, L);
   }
+}
+
+template <int N, int B>
+static cudaError_t run_fx_r2c(const FixedLaunch& L, cudaStream_t st) {
+  if constexpr (N <= 16) {
+    const int64_t blocks = (L.howmany + 255) / 256;
+    if (L.howmany > 1 && L.odist == 1)
+      return launch_pdl(fx_r2c_small_kernel<N, B, true>, dim3(unsigned(blocks)), dim3(256), 0, st, L);
+    return launch_pdl(fx_r2c_small_kernel<N, B, false>, dim3(unsigned(blocks)), dim3(256), 0, st, L);
+  } else if constexpr (N <= 256) {
+    constexpr int kThreads = 256, G = kThreads / 16;
+    const int smem = fx_smem_bytes<B>(N, G);
+    const int64_t blocks = (L.howmany + G - 1) / G;
+    return launch_pdl(fx_r2c_two_stage_kernel<N, B>, dim3(unsigned(blocks)), dim3(kThreads), size_t(smem), st, L);
+  } else {
+    const int smem = fx_smem_bytes<B>(N, 1);
+    return launch_pdl(fx_r2c_three_stage_kernel<N, B>, dim3(unsigned(L.howmany)), dim3(256), size_t(smem), st, L);
+  }
+}
+
+template <int B>
+static cudaError_t launch_fx_r2c(int n, const FixedLaunch& L, cudaStream_t st) {
+  switch (n) {
+    case 2: return run_fx_r2c<2, B>(L, st);
+    case 4: return run_fx_r2c<4, B>(L, st);
+    case 8: return run_fx_r2c<8, B>(L, st);
+    case 16: return run_fx_r2c<16, B>(L, st);
+    case 32: return run_fx_r2c<32, B>(L, st);
+    case 64: return run_fx_r2c<64, B>(L, st);
+    case 128: return run_fx_r2c<128, B>(L, st);
+    case 256: return run_fx_r2c<256, B>(L, st);
+    case 512: return run_fx_r2c<512, B>(L, st);
+    case 1024: return run_fx_r2c<1024, B>(L, st);
+    case 2048: return run_fx_r2c<2048, B>(L, st);
+    case 4096: return run_fx_r2c<4096, B>(L, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_fixed_r2c(int bits, int n, const FixedLaunch& L, cudaStream_t st) {
+  if (L.howmany > 0x7fffffffLL && n > 256) return cudaErrorInvalidValue;  // one CTA per member
+  return bits == 16 ? launch_fx_r2c<16>(n, L, st) : launch_fx_r2c<8>(n, L, st);
 }
 
 template <int B>

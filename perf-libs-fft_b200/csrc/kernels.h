@@ -318,6 +318,10 @@ struct FixedLaunch {
 };
 bool fixed_supported(int64_t n);
 cudaError_t launch_fixed(int bits, int n, int dir, const FixedLaunch& L, cudaStream_t st);
+// fixed-point R2C (forward), power-of-two n in [2, 4096]: input reals (int16
+// or int8 lanes; istride / idist in reals), output bins 0..n/2 (packed
+// complex; ostride / odist in complex elements); tw / tw2 as for the C2C
+cudaError_t launch_fixed_r2c(int bits, int n, const FixedLaunch& L, cudaStream_t st);
 
 // Split-BF16 tensor-core pass (split_bf16.cu): same addressing as a
 // four-step pass, on-chip length nl in {256, 4096} as radix-16 DFT-matrix

@@ -2,10 +2,11 @@
 //
 // The reference plans fixed-point C2C / R2C / C2R and rejects fixed-point
 // R2R (src/plfft.cpp:248-261); every fixed-point transform is scaled by
-// 1/n (docs/plfft.md:128-130).  The device path covers C2C of power-of-two
-// n <= 4096 with the reference's ESTIMATE decomposition (radix-16
-// cooley_tukey_ab, over a radix-16 cooley_tukey_ac for n > 256); other
-// fixed-point configurations fail plan creation with a reason.
+// 1/n (docs/plfft.md:128-130).  The device path covers C2C and R2C of
+// power-of-two n <= 4096 with the reference's ESTIMATE decomposition
+// (radix-16 cooley_tukey_ab, over a radix-16 cooley_tukey_ac for n > 256;
+// the R2C levels with mirrored rows); C2R and other fixed-point
+// configurations fail plan creation with a reason.
 #include <cmath>
 
 #include "plan.hpp"
@@ -37,24 +38,28 @@ static std::vector<short4> radix16_twiddles(int64_t n1, int dir, int bits) {
 
 struct FixedNode : Node {
   int bits = 16, n = 0, dir = -1;
+  bool r2c = false;
   FixedLaunch base{};
   DevBuf tw, tw2;
   cudaError_t run(const void* in, void* out, void*, cudaStream_t st) const override {
     FixedLaunch L = base;
     L.in = in;
     L.out = out;
-    return launch_fixed(bits, n, dir, L, st);
+    return r2c ? launch_fixed_r2c(bits, n, L, st) : launch_fixed(bits, n, dir, L, st);
   }
   std::string describe() const override {
     const char* shape = n <= 16 ? " one codelet" : (n <= 256 ? " 16-column x twiddled-row codelets"
                                                               : " 256-column codelets, radix-16 ac and ab levels");
-    return std::string("(c2c-") + (bits == 16 ? "q15" : "q7") + " n=" + std::to_string(n) + shape + ")";
+    return std::string(r2c ? "(r2c-" : "(c2c-") + (bits == 16 ? "q15" : "q7") + " n=" + std::to_string(n) + shape +
+           (r2c ? ", mirrored rows" : "") + ")";
   }
 };
 
-std::unique_ptr<Node> make_fixed_node(int bits, int64_t n, const Layout& lay, int dir, std::string* why) {
-  if (!fixed_supported(n)) {
-    if (why) *why = "fixed-point C2C on the device covers power-of-two n <= 4096";
+// kind: 0 C2C (dir as given), 1 R2C (forward; input reals, output bins
+// 0..n/2)
+std::unique_ptr<Node> make_fixed_node(int bits, int64_t n, const Layout& lay, int dir, std::string* why, int kind) {
+  if (!fixed_supported(n) || (kind == 1 && n < 2)) {
+    if (why) *why = "fixed-point C2C / R2C on the device cover power-of-two n <= 4096 (R2C: n >= 2)";
     return nullptr;
   }
   if (n > 256 && lay.howmany > 0x7fffffffLL) {
@@ -64,7 +69,9 @@ std::unique_ptr<Node> make_fixed_node(int bits, int64_t n, const Layout& lay, in
   auto node = std::make_unique<FixedNode>();
   node->bits = bits;
   node->n = int(n);
-  node->dir = dir;
+  node->r2c = kind == 1;
+  node->dir = kind == 1 ? -1 : dir;
+  dir = node->dir;
   node->base.howmany = lay.howmany;
   node->base.istride = lay.istride;
   node->base.idist = lay.idist;

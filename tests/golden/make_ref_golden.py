@@ -13,6 +13,12 @@ Writes:
                          inputs) plus a single-member run (the howmany = 1
                          code path)
   q7_reference.npz       the same for Q0.7
+  q15_r2c_reference.npz  Q0.15 R2C (forward), N = 2 .. 4096: 6 members
+  q7_r2c_reference.npz   (random, constants at both extremes, an impulse,
+                         alternating extremes, random extremes) per N; for
+                         N <= 256 also 32 random members; for N <= 16 also
+                         64 extreme-heavy members laid out with output
+                         distance 1 (the gu kernel variant: xu_N, yu_N)
   f32_c2c_reference.npz  FP32 C2C for a spread of lengths (single-radix,
                          two-level and three-level plans), both directions,
                          4 members of U[-1, 1) data
@@ -46,6 +52,18 @@ F32_SOURCES = ["plfft_cccn_uu.S", "plfft_cccn_uun.S", "plfft_cccn_gs.S", "plfft_
                "plfft_ab_ccct_dit_gu.S", "plfft_ab_ccct_dit_gs.S", "plfft_ac_ccct_dit_uu.S"]
 
 FIXED_SIZES = [2, 4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096]
+FIXED_REAL_SOURCES = {
+    "q15": FIXED_SOURCES["q15"] + ["plfft_q15_jjjnoh_uu.S", "plfft_q15_jjjnoh_uun.S",
+                                   "plfft_q15_hjjnoh_uu.S", "plfft_q15_hjjnoh_uun.S", "plfft_q15_hjjnoh_gs.S",
+                                   "plfft_q15_hjjnoh_gu.S", "plfft_q15_hjjnoh_us.S", "plfft_ab_q15_jjjtj_dit_gu.S",
+                                   "plfft_ab_q15_jjjtj_dit_gs.S", "plfft_ab_q15_jjjtol_dit_uun.S",
+                                   "plfft_ac_q15_jjjtj_dit_uu.S", "plfft_ac_q15_jjjtol_dit_uu.S"],
+    "q7": FIXED_SOURCES["q7"] + ["plfft_q7_pppnoh_uu.S", "plfft_q7_pppnoh_uun.S",
+                                 "plfft_q7_rppnoh_uu.S", "plfft_q7_rppnoh_uun.S", "plfft_q7_rppnoh_gs.S",
+                                 "plfft_q7_rppnoh_gu.S", "plfft_q7_rppnoh_us.S", "plfft_ab_q7_ppptj_dit_gu.S",
+                                 "plfft_ab_q7_ppptj_dit_gs.S", "plfft_ab_q7_ppptol_dit_uun.S",
+                                 "plfft_ac_q7_ppptj_dit_uu.S", "plfft_ac_q7_ppptol_dit_uu.S"],
+}
 F32_SIZES = [2, 3, 5, 7, 8, 12, 16, 20, 32, 64, 100, 128, 360, 1000, 1024, 4096]
 REAL_SIZES = [2, 3, 8, 16, 20, 64, 100, 256, 1000, 1024, 4096]
 R2R_SIZES = [16, 100, 1024]
@@ -98,6 +116,48 @@ def make_fixed(kdir, dtype, bits):
             out[f"plan_{n}_{d}"] = np.array(desc)
             print(dtype, n, d, desc, flush=True)
     np.savez_compressed(os.path.join(HERE, f"{dtype}_reference.npz"), **out)
+
+
+def fixed_real_inputs(n, hm, seed, bits):
+    lo, hi = -(1 << (bits - 1)), (1 << (bits - 1)) - 1
+    dt = np.int16 if bits == 16 else np.int8
+    rng = np.random.default_rng(seed)
+    x = rng.integers(lo, hi + 1, (hm, n)).astype(dt)
+    x[1] = hi
+    x[2] = lo
+    x[3] = 0
+    x[3, 0] = hi
+    x[4, ::2] = lo
+    x[4, 1::2] = hi
+    x[5] = np.where(rng.random(n) < 0.5, lo, hi)
+    return x
+
+
+def make_fixed_real(kdir, dtype, bits):
+    kern = neon_a64.Kernels([os.path.join(kdir, s) for s in FIXED_REAL_SOURCES[dtype]])
+    out = {}
+    for n in FIXED_SIZES:
+        hm = 32 if n <= 256 else 6
+        x = fixed_real_inputs(n, hm, (3000 if bits == 16 else 9000) + n, bits)
+        y, desc = ref_plan.run(neon_a64.Machine(kern), dtype, "r2c", -1, x.ravel(), n, hm)
+        out[f"x_{n}"], out[f"y_{n}"], out[f"plan_{n}"] = x, y.reshape(hm, n // 2 + 1, 2), np.array(desc)
+        print(dtype, "r2c", n, desc, flush=True)
+        if n <= 16:
+            # members adjacent in the output (ostride hm, odist 1): the
+            # reference's gu kernel variant, whose length-4 and length-8
+            # codelets round differently from the gs one above
+            hm = 64
+            rng = np.random.default_rng((3100 if bits == 16 else 9100) + n)
+            lo, hi = -(1 << (bits - 1)), (1 << (bits - 1)) - 1
+            ext = np.array([lo, lo + 1, hi - 1, hi])
+            xu = np.where(rng.random((hm, n)) < 0.85, rng.choice(ext, (hm, n)),
+                          rng.integers(lo, hi + 1, (hm, n))).astype(x.dtype)
+            y, desc = ref_plan.run(neon_a64.Machine(kern), dtype, "r2c", -1, xu.ravel(), n, hm,
+                                   1, n, hm, 1)
+            out[f"xu_{n}"], out[f"plan_u_{n}"] = xu, np.array(desc)
+            out[f"yu_{n}"] = np.ascontiguousarray(y.reshape(n // 2 + 1, hm, 2).transpose(1, 0, 2))
+            print(dtype, "r2c odist 1", n, desc, flush=True)
+    np.savez_compressed(os.path.join(HERE, f"{dtype}_r2c_reference.npz"), **out)
 
 
 def make_f32(kdir):
@@ -190,7 +250,7 @@ def make_real(kdir):
 
 def main():
     kdir = os.path.join(sys.argv[1], "src", "providers", "aot", "asm", "neon")
-    which = sys.argv[2:] or ["q15", "q7", "f32", "real"]
+    which = sys.argv[2:] or ["q15", "q7", "f32", "real", "q15r", "q7r"]
     if "q15" in which:
         make_fixed(kdir, "q15", 16)
     if "q7" in which:
@@ -199,6 +259,10 @@ def main():
         make_f32(kdir)
     if "real" in which:
         make_real(kdir)
+    if "q15r" in which:
+        make_fixed_real(kdir, "q15", 16)
+    if "q7r" in which:
+        make_fixed_real(kdir, "q7", 8)
 
 
 if __name__ == "__main__":
