@@ -674,9 +674,85 @@ class Q15Workload(PlanWorkload):
             def check(ref):
                 bad = int(np.count_nonzero(np.any(y != ref, axis=(1, 2))))
                 return {"members": m, "mismatched_members": bad, "bit_exact": bad == 0, "ok": bad == 0,
-                        "against": "bit-exact Q0.15 restatement (oracle/q15.c)"}
+                        "against": "bit-exact Q0.15 restatement (oracle/fixed.c)"}
         return (lambda: oracle.q15_c2c(x, -1), self.algo_bytes() * m / self.batch,
-                f"{m} of {self.batch} transforms, bit-exact Q0.15 C restatement (oracle/q15.c, 1 thread)", check)
+                f"{m} of {self.batch} transforms, bit-exact Q0.15 C restatement (oracle/fixed.c, {threads} threads)", check)
+
+
+class Q15RealWorkload(PlanWorkload):
+    """Q0.15 fixed-point R2C (int16 reals in, bins 0..N/2 as int16 re/im
+    pairs out, scaled by 1/N)."""
+
+    dtype = "int16"
+    data = "synthetic (seeded int16 reals uniform in [-2^15, 2^15))"
+
+    def __init__(self, name, desc, n, batch):
+        super().__init__(name, desc, "r2c", n, batch, profile="fx_r2c_two_stage_q15_n256_b16384")
+
+    def sizes(self):
+        return self.n * self.batch * 2, (self.n // 2 + 1) * self.batch * 4
+
+    def config(self):
+        c = super().config()
+        c["precision"] = "q15 (bit-exact to the reference's fixed-point real-input plans)"
+        return c
+
+    def setup(self, gen):
+        import torch
+
+        import plfft
+
+        self.plan = plfft.make_plan("r2c", self.n, self.batch, data_type=plfft.DataType.Q15)
+        ib, ob = self.sizes()
+        self.sets = max(2, -(-4 * L2_BYTES // (ib + ob)))
+        self.ins = [torch.randint(-(1 << 15), 1 << 15, (ib // 2,), dtype=torch.int16, device="cuda", generator=gen)
+                    for _ in range(self.sets)]
+        self.outs = [torch.empty(ob // 4, dtype=torch.int32, device="cuda") for _ in range(self.sets)]
+        self.ws = torch.empty(1, dtype=torch.uint8, device="cuda")
+        self.launches = self.plan.launch_count()
+
+    def e2e(self, steps):
+        import torch
+
+        ib, ob = self.sizes()
+        hx = self.ins[0].cpu().pin_memory()
+        hy = torch.empty(ob // 4, dtype=torch.int32).pin_memory()
+        self.plan.execute(hx.data_ptr(), hy.data_ptr())
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(torch.cuda.default_stream())
+        for _ in range(steps):
+            self.plan.execute(hx.data_ptr(), hy.data_ptr())
+        e1.record(torch.cuda.default_stream())
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, ib, ob, "plfft_plan_execute(host pinned buffers)"
+
+    def cpu_sample(self, threads, from_device=False):
+        import numpy as np
+        import torch
+
+        import oracle
+
+        idx = spread_members(self.batch, min(self.batch, 4096))
+        m = len(idx)
+        h = self.n // 2 + 1
+        y = None
+        if from_device:
+            k = self.last_set
+            sel = torch.as_tensor(idx, device="cuda", dtype=torch.int64)
+            x = self.ins[k].view(-1, self.n).index_select(0, sel).cpu().numpy()
+            y = _rows(self.outs[k], idx, h, np.int16)
+        else:
+            rng = np.random.default_rng(0)
+            x = rng.integers(-(1 << 15), 1 << 15, (m, self.n)).astype(np.int16)
+        check = None
+        if y is not None:
+            def check(ref):
+                bad = int(np.count_nonzero(np.any(y != ref, axis=(1, 2))))
+                return {"members": m, "mismatched_members": bad, "bit_exact": bad == 0, "ok": bad == 0,
+                        "against": "bit-exact Q0.15 restatement (oracle/fixed.c)"}
+        return (lambda: oracle.q15_r2c(x), self.algo_bytes() * m / self.batch,
+                f"{m} of {self.batch} transforms, bit-exact Q0.15 C restatement (oracle/fixed.c, {threads} threads)", check)
 
 
 def make_workload(name):
@@ -705,6 +781,8 @@ def make_workload(name):
         "grouped_4000": lambda: GroupedWorkload(),
         "grouped_4000_per_length": lambda: GroupedWorkload(per_length=True),
         "q15_n256_b16384": lambda: Q15Workload("q15_n256_b16384", "C2C Q0.15 forward N=256 batch=16384", 256, 16384),
+        "q15_r2c_n256_b16384": lambda: Q15RealWorkload("q15_r2c_n256_b16384", "R2C Q0.15 N=256 batch=16384", 256,
+                                                       16384),
         "diff_r2c_n8192_b1024": lambda: AdjointWorkload(),
         # kernel-coverage workloads (not benchmark configurations): the
         # smooth non-power-of-two, Rader, Bluestein and real-wrap schedules
@@ -723,7 +801,7 @@ def make_workload(name):
 WORKLOAD_NAMES = ["c2c_n1024_b4096", "r2c_c2r_n4096_b8192", "dct2_n1024_b4096", "dst2_n1024_b4096", "c2c_n1m_b64",
                   "c2c_n64k_b1024", "c2c_n1m_b64_split_bf16", "c2c_n64k_b1024_split_bf16", "grouped_4000",
                   "grouped_4000_per_length",
-                  "diff_r2c_n8192_b1024", "q15_n256_b16384",
+                  "diff_r2c_n8192_b1024", "q15_n256_b16384", "q15_r2c_n256_b16384",
                   "c2c_n1000_b16384", "c2c_n1009_b8192", "c2c_n1031_b8192", "r2c_n1000_b16384"]
 
 

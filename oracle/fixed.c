@@ -1,6 +1,6 @@
 /*
- * Bit-exact CPU restatement of the reference's fixed-point C2C path, Q0.15
- * and Q0.7 -- TEST INFRASTRUCTURE ONLY (same rules as oracle.c: only tests/
+ * Bit-exact CPU restatement of the reference's fixed-point C2C and R2C
+ * paths, Q0.15 and Q0.7 -- TEST INFRASTRUCTURE ONLY (same rules as oracle.c: only tests/
  * and the CPU-baseline leg of bench.py load it, to check results).
  *
  * What is restated (arm/perf-libs-fft), for lanes of B = 16 or 8 bits:
@@ -49,10 +49,13 @@
  * outputs of the reference's own NEON kernels composed as its ESTIMATE
  * plans (executed from their source text by tests/golden/neon_a64.py);
  * tests/test_q15.py and tests/test_q7.py require this file to match them
- * bit for bit.
+ * bit for bit; q15_r2c_reference.npz and q7_r2c_reference.npz pin the R2C
+ * (fixed_r2c below) the same way (tests/test_fixed_r2c.py).
  *
  * Data: interleaved (re, im) of int16 (Q0.15) or int8 (Q0.7), members
- * idist/odist complex elements apart, unit element stride.
+ * idist/odist complex elements apart, unit element stride (R2C: real
+ * inputs and complex outputs with their own strides).  Members are
+ * independent: the batch loops run OpenMP-parallel.
  */
 #include <math.h>
 #include <stdint.h>
@@ -304,6 +307,7 @@ static int fixed_c2c(int bits, const void *in, void *out, int64_t n, int64_t how
   const size_t esz = (size_t)(bits / 4); /* bytes per complex element */
   if (n <= 16) {
     const int s = ilog2((int)n);
+#pragma omp parallel for schedule(static)
     for (int64_t b = 0; b < howmany; ++b) {
       fc a[16], y[16];
       const void *x = (const char *)in + esz * (size_t)(b * idist);
@@ -323,10 +327,13 @@ static int fixed_c2c(int bits, const void *in, void *out, int64_t n, int64_t how
   const int sf = ilog2((int)first);
   int32_t *w = (int32_t *)malloc(sizeof(int32_t) * 4 * 15 * (size_t)(m > 1 ? m - 1 : 1));
   int32_t *w2 = (int32_t *)malloc(sizeof(int32_t) * 4 * 15 * (size_t)(m2 > 1 ? m2 - 1 : 1));
-  fc *b1 = (fc *)malloc(sizeof(fc) * (size_t)n);
-  fc *b0 = (fc *)malloc(sizeof(fc) * (size_t)n);
   twiddles16(f, m, dir, w);
   if (m2) twiddles16(f, m2, dir, w2);
+#pragma omp parallel
+  {
+  fc *b1 = (fc *)malloc(sizeof(fc) * (size_t)n); /* per-thread scratch */
+  fc *b0 = (fc *)malloc(sizeof(fc) * (size_t)n);
+#pragma omp for schedule(static)
   for (int64_t b = 0; b < howmany; ++b) {
     const void *x = (const char *)in + esz * (size_t)(b * idist);
     void *yb = (char *)out + esz * (size_t)(b * odist);
@@ -357,10 +364,11 @@ static int fixed_c2c(int bits, const void *in, void *out, int64_t n, int64_t how
       for (int k = 0; k < 16; ++k) st(bits, yb, j + m * k, y[k]);
     }
   }
-  free(w);
-  free(w2);
   free(b1);
   free(b0);
+  }
+  free(w);
+  free(w2);
   return 0;
 }
 
@@ -480,19 +488,21 @@ static int fixed_r2c(int bits, const void *in, void *out, int64_t n, int64_t how
   const fmt F = make_fmt(bits), *f = &F;
   const size_t esz = (size_t)(bits / 4), rsz = (size_t)(bits / 8);
   const int64_t h = n / 2 + 1;
-  fc *x = (fc *)malloc(sizeof(fc) * (size_t)n);
-  fc *y = (fc *)malloc(sizeof(fc) * (size_t)n);
   int32_t *w = NULL, *w2 = NULL;
-  fc *b1 = NULL, *b0 = NULL;
   const int64_t m = n / 16, m2 = n > 256 ? n / 256 : 0, first = n > 256 ? m2 : m, cols = n > 16 ? n / first : 0;
   if (n > 16) {
     w = (int32_t *)malloc(sizeof(int32_t) * 4 * 15 * (size_t)(m > 1 ? m - 1 : 1));
     w2 = (int32_t *)malloc(sizeof(int32_t) * 4 * 15 * (size_t)(m2 > 1 ? m2 - 1 : 1));
-    b1 = (fc *)malloc(sizeof(fc) * (size_t)n);
-    b0 = (fc *)malloc(sizeof(fc) * (size_t)n);
     twiddles16(f, m, -1, w);
     if (m2) twiddles16(f, m2, -1, w2);
   }
+#pragma omp parallel
+  {
+  fc *x = (fc *)malloc(sizeof(fc) * (size_t)n); /* per-thread scratch */
+  fc *y = (fc *)malloc(sizeof(fc) * (size_t)n);
+  fc *b1 = (fc *)malloc(sizeof(fc) * (size_t)n);
+  fc *b0 = (fc *)malloc(sizeof(fc) * (size_t)n);
+#pragma omp for schedule(static)
   for (int64_t b = 0; b < howmany; ++b) {
     for (int64_t k = 0; k < n; ++k) {
       const char *p = (const char *)in + rsz * (size_t)(b * idist + k * istride);
@@ -538,10 +548,11 @@ static int fixed_r2c(int bits, const void *in, void *out, int64_t n, int64_t how
   }
   free(x);
   free(y);
-  free(w);
-  free(w2);
   free(b1);
   free(b0);
+  }
+  free(w);
+  free(w2);
   return 0;
 }
 

@@ -501,41 +501,83 @@ __global__ void __launch_bounds__(256) fx_r2c_small_kernel(const FixedLaunch L) 
   for (int k = 0; k <= N / 2; ++k) y[k * L.ostride] = pack<B>(r[k]);
 }
 
-// n = 16 m, m = 2..16: G = blockDim / 16 members per CTA; rows j <= m/2
+// R2C two-stage kernel geometry: 256 threads, G members per CTA so that the
+// row stage gives every thread one row (rows j <= M/2 of each member).
+// Shared memory: twiddles, the column-stage outputs (rows 0..M/2 only, one
+// pad word per 16-word row), then (16-byte aligned) the real inputs, RP
+// lanes per member; after the column stage that area holds the members'
+// output bins, H = N/2 + 1 words apart (G H words of W fit in G RP lanes
+// of S since 2 (N/2 + 1) <= N + 16).
+__host__ __device__ constexpr int fx_r2c_rows(int n) { return n / 32 + 1; }
+__host__ __device__ constexpr int fx_r2c_members(int n) { return 256 / fx_r2c_rows(n); }
+__host__ __device__ constexpr int fx_r2c_pitch(int n) { return ((17 * fx_r2c_rows(n) + 15) / 32) * 32 + 16; }
+__host__ __device__ constexpr int fx_r2c_rpitch(int n) { return n + 16; }
+template <int B>
+__host__ __device__ constexpr int fx_r2c_real_offset(int n) {
+  return (8 * 15 * (n / 16 - 1 > 0 ? n / 16 - 1 : 1) +
+          int(sizeof(typename Fx<B>::W)) * fx_r2c_members(n) * fx_r2c_pitch(n) + 15) /
+         16 * 16;
+}
+template <int B>
+__host__ __device__ constexpr int fx_r2c_smem_bytes(int n) {
+  return fx_r2c_real_offset<B>(n) + fx_r2c_members(n) * fx_r2c_rpitch(n) * int(sizeof(FxS<B>));
+}
+
+// n = 16 m, m = 2..16.  Inputs arrive by 16-byte loads when the members are
+// 16-byte aligned rows (unit istride); outputs leave as coalesced runs of
+// each member's bins.
 template <int N, int B>
 __global__ void __launch_bounds__(256) fx_r2c_two_stage_kernel(const FixedLaunch L) {
   using W = typename Fx<B>::W;
+  using S = FxS<B>;
   griddep_wait();  // launched programmatically (launch_pdl.cuh)
   griddep_launch_dependents();
-  constexpr int M = N / 16, PITCH = fx_pitch(N), ROWS = M / 2 + 1;
+  constexpr int M = N / 16, ROWS = fx_r2c_rows(N), G = fx_r2c_members(N), PITCH = fx_r2c_pitch(N);
+  constexpr int H = N / 2 + 1, RP = fx_r2c_rpitch(N);
+  static_assert(ROWS == M / 2 + 1 && G * ROWS <= 256, "geometry");
   extern __shared__ __align__(16) unsigned char fsm[];
   short4* tw = reinterpret_cast<short4*>(fsm);  // (c, s, cvt(-s), c)
   W* tile = reinterpret_cast<W*>(tw + 15 * (M - 1 > 0 ? M - 1 : 1));
-  const int G = blockDim.x / 16;
+  S* rin = reinterpret_cast<S*>(fsm + fx_r2c_real_offset<B>(N));
+  W* bins = reinterpret_cast<W*>(rin);
   const int64_t b0 = int64_t(blockIdx.x) * G;
   const int64_t left = L.howmany - b0;
   const int cnt = left < G ? int(left) : G;
-  for (int i = threadIdx.x; i < 15 * (M - 1); i += blockDim.x) tw[i] = L.tw[i];
-  const FxS<B>* in = static_cast<const FxS<B>*>(L.in);
-  for (int f = threadIdx.x; f < cnt * N; f += blockDim.x) {
-    const int g = f / N, k = f - g * N;
-    tile[g * PITCH + fx_pos(k)] = pack<B>(qc{in[(b0 + g) * L.idist + int64_t(k) * L.istride], 0});
+  for (int i = threadIdx.x; i < 15 * (M - 1); i += 256) tw[i] = L.tw[i];
+  const S* in = static_cast<const S*>(L.in);
+  constexpr int VPM = N * int(sizeof(S)) / 16;  // 16-byte vectors per member row
+  const bool vec = L.istride == 1 && (L.idist * int64_t(sizeof(S))) % 16 == 0 &&
+                   (reinterpret_cast<uintptr_t>(in) & 15) == 0;
+  if (vec) {
+    for (int f = threadIdx.x; f < cnt * VPM; f += 256) {
+      const int g = f / VPM, v = f - g * VPM;
+      const uint4 d = __ldg(reinterpret_cast<const uint4*>(in + (b0 + g) * L.idist) + v);
+      *reinterpret_cast<uint4*>(rin + g * RP + v * (16 / int(sizeof(S)))) = d;
+    }
+  } else {
+    for (int f = threadIdx.x; f < cnt * N; f += 256) {
+      const int g = f / N, k = f - g * N;
+      rin[g * RP + k] = in[(b0 + g) * L.idist + int64_t(k) * L.istride];
+    }
   }
   __syncthreads();
-  const int g = threadIdx.x >> 4, c = threadIdx.x & 15;
-  W* mine = tile + g * PITCH;
-  if (g < cnt) {  // stage 1: length-M real codelet down column c, in place
+  // stage 1: length-M real codelet down column c of member g; only the
+  // bins k <= M/2 are kept (the rows stage 2 reads)
+  for (int task = threadIdx.x; task < cnt * 16; task += 256) {
+    const int g = task >> 4, c = task & 15;
     int xr[M];
     qc r[M];
 #pragma unroll
-    for (int q = 0; q < M; ++q) xr[q] = unpack(mine[fx_pos(c + 16 * q)]).re;
+    for (int q = 0; q < M; ++q) xr[q] = rin[g * RP + c + 16 * q];
     q_real_codelet<M, B, true>(xr, r);
+    W* mine = tile + g * PITCH;
 #pragma unroll
-    for (int k = 0; k < M; ++k) mine[fx_pos(c + 16 * k)] = pack<B>(r[k]);
+    for (int k = 0; k < ROWS; ++k) mine[fx_pos(c + 16 * k)] = pack<B>(r[k]);
   }
   __syncthreads();
-  // stage 2: rows (member, j <= M/2); row M - j is the mirror of row j
-  for (int row = threadIdx.x; row < cnt * ROWS; row += blockDim.x) {
+  // stage 2: rows (member, j <= M/2); row M - j is the mirror of row j.
+  // Bins go to the shared output area (the real inputs are consumed).
+  for (int row = threadIdx.x; row < cnt * ROWS; row += 256) {
     const int gg = row / ROWS, j = row - gg * ROWS;
     const W* src = tile + gg * PITCH + fx_pos(16 * j);
     qc a[16], r[16];
@@ -545,14 +587,20 @@ __global__ void __launch_bounds__(256) fx_r2c_two_stage_kernel(const FixedLaunch
       a[i] = (i == 0 || j == 0) ? s : Ar<B>::twiddle(s, tw[15 * (j - 1) + (i - 1)]);
     }
     q_dft<16, B>(a, r);
-    W* y = static_cast<W*>(L.out) + (b0 + gg) * L.odist;
+    W* y = bins + gg * H;
     const bool mirror = j > 0 && 2 * j < M;
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
       const int t = j + M * k, tm = (M - j) + M * (15 - k);
-      if (t <= N / 2) y[int64_t(t) * L.ostride] = pack<B>(r[k]);
-      if (mirror && tm <= N / 2) y[int64_t(tm) * L.ostride] = pack<B>(fx_conj<B>(r[k]));
+      if (t <= N / 2) y[t] = pack<B>(r[k]);
+      if (mirror && tm <= N / 2) y[tm] = pack<B>(fx_conj<B>(r[k]));
     }
+  }
+  __syncthreads();
+  W* out = static_cast<W*>(L.out);
+  for (int f = threadIdx.x; f < cnt * H; f += 256) {
+    const int gg = f / H, t = f - gg * H;
+    out[(b0 + gg) * L.odist + int64_t(t) * L.ostride] = bins[gg * H + t];
   }
 }
 
@@ -659,10 +707,10 @@ static cudaError_t run_fx_r2c(const FixedLaunch& L, cudaStream_t st) {
       return launch_pdl(fx_r2c_small_kernel<N, B, true>, dim3(unsigned(blocks)), dim3(256), 0, st, L);
     return launch_pdl(fx_r2c_small_kernel<N, B, false>, dim3(unsigned(blocks)), dim3(256), 0, st, L);
   } else if constexpr (N <= 256) {
-    constexpr int kThreads = 256, G = kThreads / 16;
-    const int smem = fx_smem_bytes<B>(N, G);
+    constexpr int G = fx_r2c_members(N), smem = fx_r2c_smem_bytes<B>(N);
+    static_assert(smem <= 48 * 1024, "default dynamic shared-memory limit");
     const int64_t blocks = (L.howmany + G - 1) / G;
-    return launch_pdl(fx_r2c_two_stage_kernel<N, B>, dim3(unsigned(blocks)), dim3(kThreads), size_t(smem), st, L);
+    return launch_pdl(fx_r2c_two_stage_kernel<N, B>, dim3(unsigned(blocks)), dim3(256), size_t(smem), st, L);
   } else {
     const int smem = fx_smem_bytes<B>(N, 1);
     return launch_pdl(fx_r2c_three_stage_kernel<N, B>, dim3(unsigned(L.howmany)), dim3(256), size_t(smem), st, L);

@@ -119,6 +119,30 @@ def test_fixed_r2c_strided(dtype, n):
     assert np.array_equal(got, ref), plan.describe()
 
 
+@pytest.mark.parametrize("dtype", ["q15", "q7"])
+@pytest.mark.parametrize("n", [8, 64, 256, 1024])
+def test_fixed_r2c_in_place(dtype, n):
+    """In place over the padded layout (each member's bins over its own
+    reals, idist = 2 (n/2 + 1) reals): the same bits as out of place."""
+    import plfft
+    import torch
+
+    bits, lane, _, name = TYPES[dtype]
+    lim = 1 << (bits - 1)
+    hm, h = 300, n // 2 + 1
+    rng = np.random.default_rng(n + bits)
+    x = np.zeros((hm, 2 * h), lane)
+    x[:, :n] = rng.integers(-lim, lim, (hm, n))
+    d = torch.from_numpy(x.view(np.uint8).ravel().copy()).cuda()
+    plan = plfft.make_plan("r2c", n, hm, 1, 2 * h, 1, h, alias=plfft.IoAlias.MAY_ALIAS,
+                           data_type=plfft.DataType[name])
+    plan.execute(d.data_ptr(), d.data_ptr())
+    torch.cuda.synchronize()
+    got = d.cpu().numpy().view(lane).reshape(hm, h, 2)
+    ref = oracle.q15_r2c(x[:, :n]) if dtype == "q15" else oracle.q7_r2c(x[:, :n])
+    assert np.array_equal(got, ref), plan.describe()
+
+
 @pytest.mark.parametrize("name", ["Q15", "Q7"])
 def test_fixed_real_unsupported_configs_fail_plan_creation(name):
     """Fixed-point C2R (not built) and R2C lengths outside the powers of two

@@ -5,7 +5,7 @@ Q0.15 kernels (src/providers/aot/asm/neon/plfft_*q15*.S), executed from
 their source text by tests/golden/neon_a64.py and composed as the
 reference's ESTIMATE plan by tests/golden/ref_plan.py
 (tests/golden/make_ref_golden.py).  The C
-restatement oracle/q15.c must reproduce them bit for bit.  It must also
+restatement oracle/fixed.c must reproduce them bit for bit.  It must also
 meet the reference's own fixed-point accuracy bound: 6 * log2(n) LSB
 against the exact DFT scaled by 1/n (test/test_utils.hpp:131-152).
 """

@@ -1,6 +1,6 @@
 """Q0.15 C2C on the device (through the C-ABI) vs the reference's own
 kernels' outputs (tests/golden/q15_reference.npz) and the bit-exact oracle
-(oracle/q15.c): every case must match bit for bit.
+(oracle/fixed.c): every case must match bit for bit.
 """
 import numpy as np
 import pytest
