@@ -1033,15 +1033,20 @@ def main():
     # the timed region nothing
     sampler = ClockSampler(local)
     sampler.start()
+    # the step index picks the buffer set; it runs on through every phase so
+    # that no timed step finds its set still in L2 from an earlier one
+    nxt = 0
     for i in range(args.warmup):
-        w.step(i, sh)
+        w.step(nxt, sh)
+        nxt += 1
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if args.steps is None:
         # size the timed region to about one second (clock samples need it)
         ev0.record(stream)
         for i in range(20):
-            w.step(i, sh)
+            w.step(nxt, sh)
+            nxt += 1
         ev1.record(stream)
         torch.cuda.synchronize()
         est = ev0.elapsed_time(ev1) / 20
@@ -1056,10 +1061,12 @@ def main():
     # not the host's latency of the first launch (the host keeps ahead after
     # that: it submits a step faster than the device runs one)
     torch.cuda._sleep(QUEUE_DELAY_CYCLES)
+    first_timed = nxt
     ev0.record(stream)
     for i in range(args.steps):
-        w.step(i, sh)
+        w.step(first_timed + i, sh)
     ev1.record(stream)
+    nxt = first_timed + args.steps
     torch.cuda.synchronize()
     sampler.mark_end()
     barrier()
@@ -1070,7 +1077,7 @@ def main():
     kev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * nk)]
     for i in range(nk):
         kev[2 * i].record(stream)
-        w.step(i, sh)
+        w.step(nxt + i, sh)
         kev[2 * i + 1].record(stream)
     torch.cuda.synchronize()
     step_ms = statistics.median(kev[2 * i].elapsed_time(kev[2 * i + 1]) for i in range(nk))
@@ -1099,10 +1106,11 @@ def main():
     achieved = abytes / (kernel_ms * 1e-3) / 1e9
     cpu, parity = None, None
     if rank == 0 and not args.no_cpu_baseline:
-        # the per-step timing loop above ran steps 0..nk-1 last: redo the
-        # final timed step so the checked buffer set is the timed one's
+        # the per-step timing loop above ran other buffer sets last (and may
+        # have wrapped onto the timed one): redo the final timed step so the
+        # checked buffer set holds the timed step's outputs
         if last_timed_set is not None:
-            w.step(args.steps - 1, sh)
+            w.step(first_timed + args.steps - 1, sh)
             torch.cuda.synchronize()
         cpu, parity = cpu_baseline(w)
     if rank == 0:
