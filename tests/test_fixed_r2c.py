@@ -73,3 +73,29 @@ def test_fixed_r2c_within_float_tolerance(dtype, bits, n):
     ref = oracle.r2c(x.astype(np.float64)) / n
     err = np.abs((y[..., 0] + 1j * y[..., 1]) - ref).max()
     assert err <= 2 + np.log2(n), err
+
+
+@pytest.mark.parametrize("bits", [16, 8])
+@pytest.mark.parametrize("n", [4, 8, 64, 512])
+def test_fixed_r2c_strided_entry_matches_layout_forms(bits, n):
+    """The strided entry point agrees with the two layout forms the
+    fixtures pin: gs (contiguous members) and gu (members adjacent in the
+    output), and a gapped layout agrees with the contiguous one member by
+    member (the variant depends only on howmany and odist)."""
+    it = np.int16 if bits == 16 else np.int8
+    lim = 1 << (bits - 1)
+    hm, h = 9, n // 2 + 1
+    rng = np.random.default_rng(n + bits)
+    x = rng.integers(-lim, lim, (hm, n)).astype(it)
+    fn = oracle.q15_r2c if bits == 16 else oracle.q7_r2c
+    gs = oracle.fixed_r2c_strided(bits, x.ravel(), n, hm, 1, n, 1, h, hm * h).reshape(hm, h, 2)
+    assert np.array_equal(gs, fn(x))
+    gu = oracle.fixed_r2c_strided(bits, x.ravel(), n, hm, 1, n, hm, 1, hm * h).reshape(h, hm, 2)
+    assert np.array_equal(gu.transpose(1, 0, 2), fn(x, odist_unit=True))
+    buf = np.zeros((hm - 1) * (2 * n + 3) + 2 * (n - 1) + 1, it)
+    for b in range(hm):
+        buf[b * (2 * n + 3):b * (2 * n + 3) + 2 * n:2] = x[b]
+    od = 3 * h + 1
+    out = oracle.fixed_r2c_strided(bits, buf, n, hm, 2, 2 * n + 3, 3, od, (hm - 1) * od + 3 * (h - 1) + 1)
+    got = np.stack([out[b * od:b * od + 3 * h:3] for b in range(hm)])
+    assert np.array_equal(got, fn(x))
