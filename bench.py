@@ -688,6 +688,7 @@ class Q15RealWorkload(PlanWorkload):
 
     def __init__(self, name, desc, n, batch):
         super().__init__(name, desc, "r2c", n, batch, profile="fx_r2c_two_stage_q15_n256_b16384")
+        self.data = Q15RealWorkload.data  # the real-kind default set by the base is for float data
 
     def sizes(self):
         return self.n * self.batch * 2, (self.n // 2 + 1) * self.batch * 4
