@@ -191,6 +191,28 @@ def test_q15_n256_full_batch_bit_exact():
     assert bad.size == 0, (bad[:10], plan.describe())
 
 
+def test_q15_r2c_n256_full_batch_bit_exact():
+    """Q0.15 R2C N=256 x 16384 (the bench's R2C workload), int16 reals over
+    the full range: every member's bins bit for bit, nothing written past
+    the output."""
+    import torch
+
+    n, howmany = 256, 16384
+    h = n // 2 + 1
+    plan = plfft.make_plan("r2c", n, howmany, data_type=plfft.DataType.Q15)
+    rng = np.random.default_rng(17)
+    x = rng.integers(-(1 << 15), 1 << 15, (howmany, n)).astype(np.int16)
+    d_in = torch.from_numpy(x.reshape(-1).copy()).cuda()
+    d_out = torch.full((howmany * h + 64,), 0x5A5A5A5A, dtype=torch.int32, device="cuda")
+    plan.execute(d_in.data_ptr(), d_out.data_ptr())
+    out = d_out.cpu().numpy()
+    assert np.all(out[howmany * h:] == 0x5A5A5A5A)
+    got = out[:howmany * h].view(np.int16).reshape(howmany, h, 2)
+    ref = oracle.q15_r2c(x)
+    bad = np.nonzero(np.any(got != ref, axis=(1, 2)))[0]
+    assert bad.size == 0, (bad[:10], plan.describe())
+
+
 def _impulse_input(howmany, n, seed):
     """U[-1,1) re/im plus a +-1e3 impulse at a seeded bin per member."""
     rng = np.random.default_rng(seed)
