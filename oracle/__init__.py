@@ -146,7 +146,7 @@ def _libq():
         for name in ("oracle_q15_c2c", "oracle_q7_c2c"):
             getattr(L, name).argtypes = [dp, dp, i64, i64, i64, i64, ctypes.c_int]
             getattr(L, name).restype = ctypes.c_int
-        for name in ("oracle_q15_r2c", "oracle_q7_r2c"):
+        for name in ("oracle_q15_r2c", "oracle_q7_r2c", "oracle_q15_c2r", "oracle_q7_c2r"):
             getattr(L, name).argtypes = [dp, dp, i64, i64, i64, i64, i64, i64]
             getattr(L, name).restype = ctypes.c_int
         L.oracle_q15_twiddles.argtypes = [i64, ctypes.c_int, dp]
@@ -216,6 +216,33 @@ def q7_r2c(x, odist_unit=False):
     """x: int8 [howmany, n] reals -> int8 [howmany, n/2+1, 2], scaled by 1/n.
     odist_unit: compute as a batch laid out with output distance 1."""
     return _fixed_r2c(x, np.int8, _libq().oracle_q7_r2c, odist_unit)
+
+
+def fixed_c2r_strided(bits, buf, n, howmany, istride, idist, ostride, odist, out_elems):
+    """C2R of the members of the flat buffer buf of complex lanes ([elements,
+    2], int16 for bits 16, int8 for 8) in the given layout; returns the flat
+    real output [out_elems] (zero where no output lands)."""
+    dtype = np.int16 if bits == 16 else np.int8
+    buf = np.ascontiguousarray(buf, dtype=dtype)
+    y = np.zeros(out_elems, dtype)
+    fn = _libq().oracle_q15_c2r if bits == 16 else _libq().oracle_q7_c2r
+    if fn(_ptr(buf), _ptr(y), n, howmany, istride, idist, ostride, odist) != 0:
+        raise ValueError(f"fixed-point oracle: unsupported length {n}")
+    return y
+
+
+def q15_c2r(X, n):
+    """X: int16 [howmany, n/2+1, 2] bins -> int16 [howmany, n] reals, scaled by 1/n."""
+    X = np.ascontiguousarray(X, dtype=np.int16)
+    hm = X.shape[0]
+    return fixed_c2r_strided(16, X, n, hm, 1, n // 2 + 1, 1, n, hm * n).reshape(hm, n)
+
+
+def q7_c2r(X, n):
+    """X: int8 [howmany, n/2+1, 2] bins -> int8 [howmany, n] reals, scaled by 1/n."""
+    X = np.ascontiguousarray(X, dtype=np.int8)
+    hm = X.shape[0]
+    return fixed_c2r_strided(8, X, n, hm, 1, n // 2 + 1, 1, n, hm * n).reshape(hm, n)
 
 
 def q15_twiddles(n, direction=-1):

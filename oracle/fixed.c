@@ -556,6 +556,246 @@ static int fixed_r2c(int bits, const void *in, void *out, int64_t n, int64_t how
   return 0;
 }
 
+/* ---- C2R (backward), the reference's fixed-point real-output plans ----
+ *
+ * The C2R plan is the C2C decomposition run backward with decimation in
+ * frequency (planner/strategies/cooley_tukey.hpp:250-323, 498-580; the
+ * level call sequences of src/level_ab_t_c2r.cpp:17-99 and
+ * src/level_ac_t_c2r.cpp:17-100):
+ *   N <= 16       one real-output codelet;
+ *   N = 16 m      a radix-16 DIF level over rows j = 0..m/2 of the Hermitian
+ *                 input (row j: inputs X[j + m i], i = 0..15, those past the
+ *                 stored half read as conjugates, X[j + m i] = conj(X[m (16 -
+ *                 i) - j]); a backward 16-point codelet; outputs k >= 1 of
+ *                 rows j >= 1 times W_N^{jk}) into b[16 j + k], then per
+ *                 column k a real-output codelet of length m over b[16 j + k],
+ *                 j = 0..m/2, giving x[k + 16 t];
+ *   N = 256 m'    the same first level, then per column k a second radix-16
+ *                 DIF level over rows i = 0..m'/2 of that column's length-m
+ *                 Hermitian sequence into c[256 i + 16 q + k], then per lane
+ *                 l < 256 a real-output codelet of length m' over
+ *                 c[256 i + l], giving x[l + 256 t].
+ * Rows j = m/2 + 1..m - 1 are not needed: the column sequences are
+ * Hermitian, and each codelet conjugates what it needs.
+ * Rounding, read from the kernels (plfft_*_q15_jjjnbih_*,
+ * plfft_ab/ac_16_q15_jjjtbil_dif_*, plfft_*_q15_jjhnb_*; the q7 ones follow
+ * the same dataflow): inputs are pre-shifted by log2 of the codelet length
+ * first, and a conjugated input is then (rdm(re, 1), rdm(im, -1)); the row
+ * kernels are then exactly the backward complex codelet on that column and
+ * the DIF twiddle the premultiplied two-product MAC; the real-output
+ * codelets of lengths 2 and 4 are the real parts of the backward complex
+ * codelet, and those of lengths 8 and 16 round their constant products in
+ * their own places (real_out8, real_out16). */
+
+/* the length-r column with conjugate extension: element e of the stored
+ * half is X[e * xs] (e <= r/2, or e <= h for the row form below) */
+static fc cx_in(const fmt *f, fc v, int s, int conj) {
+  const fc a = {s ? rshr(v.re, s) : v.re, s ? rshr(v.im, s) : v.im};
+  return conj ? (fc){rdm(f, a.re, f->one), rdm(f, a.im, f->mone)} : a;
+}
+
+/* real-output codelet of length 8 on the extended, pre-shifted inputs A */
+static void real_out8(const fmt *f, const fc *A, int32_t *x) {
+  const int32_t s04 = sat(f, A[0].re + A[4].re), d04 = sat(f, A[0].re - A[4].re);
+  const int32_t s26 = sat(f, A[2].re + A[6].re), e26 = sat(f, A[2].im - A[6].im);
+  const fc p15 = {sat(f, A[1].re - A[5].re), sat(f, A[1].im - A[5].im)};
+  const fc p37 = {sat(f, A[3].re - A[7].re), sat(f, A[3].im - A[7].im)};
+  const int32_t qr = sat(f, sat(f, A[1].re + A[5].re) + sat(f, A[3].re + A[7].re));
+  const int32_t qi = sat(f, sat(f, A[1].im + A[5].im) - sat(f, A[3].im + A[7].im));
+  const int32_t u = rdm(f, sat(f, p15.re - p37.re), f->c8); /* c8 (a - b), one rounding */
+  const int32_t v = rdm(f, sat(f, p15.im + p37.im), f->c8);
+  const int32_t e = sat(f, s04 + s26), g = sat(f, s04 - s26);
+  const int32_t a = sat(f, d04 + u), b = sat(f, sat(f, -(int64_t)e26) - v);
+  const int32_t c = sat(f, d04 - u), d = sat(f, v - e26);
+  x[0] = sat(f, e + qr);
+  x[4] = sat(f, e - qr);
+  x[2] = sat(f, g - qi);
+  x[6] = sat(f, g + qi);
+  x[1] = sat(f, a + b);
+  x[7] = sat(f, a - b);
+  x[3] = sat(f, c - d);
+  x[5] = sat(f, c + d);
+}
+
+/* real-output codelet of length 16 on the extended, pre-shifted inputs A:
+ * the split-radix real parts; the odd quarter-wave terms are rotated by
+ * pairs of two-product MACs, the eighth-wave terms by a rounded c8 product
+ * folded into a MAC with the unit constant */
+static void real_out16(const fmt *f, const fc *A, int32_t *x) {
+#define SA(a, b) sat(f, (int64_t)(a) + (b))
+#define SS(a, b) sat(f, (int64_t)(a) - (b))
+  const int32_t C8 = f->c8, C16 = f->c16, S16 = f->s16, HI = f->one, LO = f->mone;
+  /* even half: inputs 0, 2, ..., 14 */
+  const int32_t s08 = SA(A[0].re, A[8].re), d08 = SS(A[0].re, A[8].re);
+  const int32_t s4c = SA(A[4].re, A[12].re), d4c = SS(A[4].im, A[12].im);
+  const int32_t ev = SA(s08, s4c), ew = SS(s08, s4c);
+  const int32_t s2a6e = SA(SA(A[2].re, A[10].re), SA(A[6].re, A[14].re));
+  const int32_t r2a = SS(A[2].re, A[10].re), i2a = SS(A[2].im, A[10].im);
+  const int32_t r6e = SS(A[6].re, A[14].re), i6e = SS(A[6].im, A[14].im);
+  const int32_t i26 = SS(SA(A[2].im, A[10].im), SA(A[6].im, A[14].im));
+  const int32_t e0 = SA(ev, s2a6e), e4 = SS(ev, s2a6e);
+  const int32_t f1 = SS(d08, d4c), f3 = SA(d08, d4c);
+  const int32_t f2 = SS(ew, i26), f6 = SA(ew, i26);
+  /* odd half: inputs 1, 3, ..., 15 */
+  const int32_t s19 = SA(A[1].re, A[9].re), s5d = SA(A[5].re, A[13].re);
+  const int32_t s3b = SA(A[3].re, A[11].re), s7f = SA(A[7].re, A[15].re);
+  const int32_t o0 = SA(SA(s19, s5d), SA(s3b, s7f));
+  const int32_t i3b = SS(A[3].im, A[11].im), r7f = rdm(f, SS(A[7].re, A[15].re), HI);
+  const int32_t r3b = SS(A[3].re, A[11].re), i7f = rdm(f, SS(A[7].im, A[15].im), LO);
+  const int32_t i19 = SS(A[1].im, A[9].im), r5d = rdm(f, SS(A[5].re, A[13].re), HI);
+  const int32_t r19 = SS(A[1].re, A[9].re), i5d = rdm(f, SS(A[5].im, A[13].im), LO);
+  const int32_t p3 = SA(i3b, r7f), q3 = SA(r3b, i7f), p1 = SA(i19, r5d), q1 = SA(r19, i5d);
+  const int32_t m3 = SS(i3b, r7f), n3 = SS(r3b, i7f), m1 = SS(i19, r5d), n1 = SS(r19, i5d);
+  const int32_t j3b = SA(A[3].im, A[11].im), j7f = SA(A[7].im, A[15].im), j37 = SS(j3b, j7f);
+  const int32_t k37 = SS(s3b, s7f);
+  const int32_t j19 = SA(A[1].im, A[9].im), j5d = SA(A[5].im, A[13].im), j15 = SS(j19, j5d);
+  const int32_t k15 = SS(s19, s5d);
+  const int32_t o4 = SS(SA(j19, j5d), SA(j3b, j7f));
+  /* rotations */
+  const int32_t w1 = rdm(f, SS(mac2(f, i6e, -C8, rdm(f, r6e, -C8), HI), mac2(f, i2a, C8, rdm(f, r2a, C8), LO)), LO);
+  const int32_t w3 = SA(mac2(f, r2a, C8, rdm(f, i2a, C8), HI), mac2(f, r6e, -C8, rdm(f, i6e, -C8), LO));
+  const int32_t z2 = rdm(f, SS(mac2(f, j37, -C8, rdm(f, k37, -C8), HI), mac2(f, j15, C8, rdm(f, k15, C8), LO)), LO);
+  const int32_t z6 = SA(mac2(f, k15, C8, rdm(f, j15, C8), HI), mac2(f, k37, -C8, rdm(f, j37, -C8), LO));
+  const int32_t z1 = rdm(f, SS(mac2(f, p3, -C16, q3, S16), mac2(f, p1, S16, q1, -C16)), LO);
+  const int32_t z3 = rdm(f, SS(mac2(f, m3, S16, n3, -C16), mac2(f, m1, C16, n1, -S16)), LO);
+  const int32_t z5 = SA(mac2(f, q1, S16, p1, C16), mac2(f, q3, -C16, p3, -S16));
+  const int32_t z7 = SA(mac2(f, n1, C16, m1, S16), mac2(f, n3, S16, m3, C16));
+  const int32_t g1 = SS(f1, w1), g5 = SA(f1, w1), g3 = SS(f3, w3), g7 = SA(f3, w3);
+  x[0] = SA(e0, o0);
+  x[8] = SS(e0, o0);
+  x[4] = SS(e4, o4);
+  x[12] = SA(e4, o4);
+  x[2] = SS(f2, z2);
+  x[10] = SA(f2, z2);
+  x[6] = SS(f6, z6);
+  x[14] = SA(f6, z6);
+  x[1] = SS(g1, z1);
+  x[9] = SA(g1, z1);
+  x[3] = SS(g3, z3);
+  x[11] = SA(g3, z3);
+  x[5] = SS(g5, z5);
+  x[13] = SA(g5, z5);
+  x[7] = SS(g7, z7);
+  x[15] = SA(g7, z7);
+#undef SA
+#undef SS
+}
+
+/* real-output codelet of length r (2..16) over the Hermitian half
+ * X[e * xs], e = 0..r/2 */
+static void real_out(const fmt *f, int r, const fc *X, int64_t xs, int32_t *x) {
+  const int s = ilog2(r);
+  fc A[16] = {{0, 0}}, y[16];
+  for (int i = 0; i < r; ++i) A[i] = i <= r / 2 ? cx_in(f, X[i * xs], s, 0) : cx_in(f, X[(r - i) * xs], s, 1);
+  if (r == 8) {
+    real_out8(f, A, x);
+  } else if (r == 16) {
+    real_out16(f, A, x);
+  } else {
+    codelet(f, r, 1, A, y);
+    for (int k = 0; k < r; ++k) x[k] = y[k].re;
+  }
+}
+
+/* row j of a radix-16 DIF level over `rows` rows of a Hermitian sequence
+ * of length 16 rows (stored half X[e * xs], e = 0..8 rows): the 16 outputs,
+ * twiddled by W_{16 rows}^{jk} (w: the backward table over `rows` rows) */
+static void dif_row(const fmt *f, const fc *X, int64_t xs, int64_t rows, int64_t j, const int32_t *w, fc *y) {
+  fc a[16], t[16];
+  for (int i = 0; i < 16; ++i) {
+    const int direct = j == 0 ? i <= 8 : i <= 7;
+    a[i] = direct ? cx_in(f, X[(j + rows * i) * xs], 4, 0) : cx_in(f, X[(rows * (16 - i) - j) * xs], 4, 1);
+  }
+  codelet(f, 16, 1, a, t);
+  for (int k = 0; k < 16; ++k) {
+    if (j > 0 && k > 0) {
+      const int32_t *c = w + 4 * (15 * (j - 1) + (k - 1));
+      y[k] = (fc){mac2(f, t[k].re, c[0], t[k].im, c[2]), mac2(f, t[k].re, c[1], t[k].im, c[3])};
+    } else {
+      y[k] = t[k];
+    }
+  }
+}
+
+/* fixed-point C2R (backward) of power-of-two n in [2, 4096]: inputs bins
+ * 0..n/2 (istride / idist in complex elements), outputs n reals (ostride /
+ * odist in reals), scaled by 1/n */
+static int fixed_c2r(int bits, const void *in, void *out, int64_t n, int64_t howmany, int64_t istride,
+                     int64_t idist, int64_t ostride, int64_t odist) {
+  if (n < 2 || n > 4096 || (n & (n - 1))) return -1;
+  const fmt F = make_fmt(bits), *f = &F;
+  const size_t esz = (size_t)(bits / 4), rsz = (size_t)(bits / 8);
+  const int64_t h = n / 2 + 1, m = n / 16, m2 = n > 256 ? n / 256 : 0;
+  int32_t *w = NULL, *w2 = NULL;
+  if (n > 16) {
+    w = (int32_t *)malloc(sizeof(int32_t) * 4 * 15 * (size_t)(m > 1 ? m - 1 : 1));
+    twiddles16(f, m, 1, w);
+  }
+  if (m2) {
+    w2 = (int32_t *)malloc(sizeof(int32_t) * 4 * 15 * (size_t)(m2 > 1 ? m2 - 1 : 1));
+    twiddles16(f, m2, 1, w2);
+  }
+#pragma omp parallel
+  {
+  fc *X = (fc *)malloc(sizeof(fc) * (size_t)h); /* per-thread scratch */
+  fc *b = (fc *)malloc(sizeof(fc) * (size_t)n);
+  fc *c = (fc *)malloc(sizeof(fc) * (size_t)n);
+  int32_t *x = (int32_t *)malloc(sizeof(int32_t) * (size_t)n);
+#pragma omp for schedule(static)
+  for (int64_t mb = 0; mb < howmany; ++mb) {
+    for (int64_t k = 0; k < h; ++k) X[k] = ld(bits, (const char *)in + esz * (size_t)(mb * idist + k * istride), 0);
+    if (n <= 16) {
+      real_out(f, (int)n, X, 1, x);
+    } else {
+      for (int64_t j = 0; j <= m / 2; ++j) dif_row(f, X, 1, m, j, w, b + 16 * j);
+      if (!m2) {
+        for (int k = 0; k < 16; ++k) {
+          int32_t col[16];
+          real_out(f, (int)m, b + k, 16, col);
+          for (int64_t t = 0; t < m; ++t) x[k + 16 * t] = col[t];
+        }
+      } else {
+        for (int k = 0; k < 16; ++k)
+          for (int64_t i = 0; i <= m2 / 2; ++i) {
+            fc y[16];
+            dif_row(f, b + k, 16, m2, i, w2, y);
+            for (int q = 0; q < 16; ++q) c[256 * i + 16 * q + k] = y[q];
+          }
+        for (int l = 0; l < 256; ++l) {
+          int32_t col[16];
+          real_out(f, (int)m2, c + l, 256, col);
+          for (int64_t t = 0; t < m2; ++t) x[l + 256 * t] = col[t];
+        }
+      }
+    }
+    for (int64_t t = 0; t < n; ++t) {
+      char *p = (char *)out + rsz * (size_t)(mb * odist + t * ostride);
+      if (bits == 16)
+        *(int16_t *)p = (int16_t)x[t];
+      else
+        *(int8_t *)p = (int8_t)x[t];
+    }
+  }
+  free(X);
+  free(b);
+  free(c);
+  free(x);
+  }
+  free(w);
+  free(w2);
+  return 0;
+}
+
+int oracle_q15_c2r(const int16_t *in, int16_t *out, int64_t n, int64_t howmany, int64_t istride, int64_t idist,
+                   int64_t ostride, int64_t odist) {
+  return fixed_c2r(16, in, out, n, howmany, istride, idist, ostride, odist);
+}
+
+int oracle_q7_c2r(const int8_t *in, int8_t *out, int64_t n, int64_t howmany, int64_t istride, int64_t idist,
+                  int64_t ostride, int64_t odist) {
+  return fixed_c2r(8, in, out, n, howmany, istride, idist, ostride, odist);
+}
+
 int oracle_q15_r2c(const int16_t *in, int16_t *out, int64_t n, int64_t howmany, int64_t istride, int64_t idist,
                    int64_t ostride, int64_t odist) {
   return fixed_r2c(16, in, out, n, howmany, istride, idist, ostride, odist);

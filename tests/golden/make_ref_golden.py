@@ -13,6 +13,11 @@ Writes:
                          inputs) plus a single-member run (the howmany = 1
                          code path)
   q7_reference.npz       the same for Q0.7
+  q15_c2r_reference.npz  Q0.15 / Q0.7 C2R (backward), N = 2 .. 4096: 32
+  q7_c2r_reference.npz   members (N <= 256) or 6, Hermitian half spectra
+                         with random, extreme, zero and constant bins; for
+                         N <= 256 also the same members laid out adjacent
+                         (the batched plans: yu_N)
   q15_r2c_reference.npz  Q0.15 R2C (forward), N = 2 .. 4096: 6 members
   q7_r2c_reference.npz   (random, constants at both extremes, an impulse,
                          alternating extremes, random extremes) per N; for
@@ -30,6 +35,7 @@ Writes:
                          455-469, 686-701, 828-854); the permutation and
                          rotation are restated here in single precision
 """
+import glob
 import os
 import sys
 
@@ -160,6 +166,36 @@ def make_fixed_real(kdir, dtype, bits):
     np.savez_compressed(os.path.join(HERE, f"{dtype}_r2c_reference.npz"), **out)
 
 
+def make_fixed_c2r(kdir, dtype, bits):
+    """Fixed-point C2R (backward): the reference's real-output plans on
+    Hermitian half spectra (random, extremes, zero and constant bins), for
+    N = 2..4096; for N <= 256 also a batch laid out with members adjacent
+    (istride = howmany, idist = 1: the batched AC plans)."""
+    kern = neon_a64.Kernels(sorted(glob.glob(os.path.join(kdir, f"*{dtype}*.S"))))
+    lo, hi = -(1 << (bits - 1)), (1 << (bits - 1)) - 1
+    it = np.int16 if bits == 16 else np.int8
+    out = {}
+    for n in FIXED_SIZES:
+        h = n // 2 + 1
+        hm = 32 if n <= 256 else 6
+        rng = np.random.default_rng((5000 if bits == 16 else 7000) + n)
+        X = np.where(rng.random((hm, h, 2)) < 0.6, rng.choice([lo, hi, lo + 1, hi - 1, 0], (hm, h, 2)),
+                     rng.integers(lo, hi + 1, (hm, h, 2))).astype(it)
+        X[1] = 0
+        X[1, 0, 0] = hi  # a constant signal
+        X[2] = hi
+        X[3] = lo
+        y, desc = ref_plan.run(neon_a64.Machine(kern), dtype, "c2r", 1, X.ravel(), n, hm)
+        out[f"x_{n}"], out[f"y_{n}"], out[f"plan_{n}"] = X, y.reshape(hm, n), np.array(desc)
+        print(dtype, "c2r", n, desc, flush=True)
+        if n <= 256:
+            buf = np.ascontiguousarray(X.transpose(1, 0, 2))  # element k of member b at k * hm + b
+            y, desc = ref_plan.run(neon_a64.Machine(kern), dtype, "c2r", 1, buf.ravel(), n, hm, hm, 1, hm, 1)
+            out[f"yu_{n}"], out[f"plan_u_{n}"] = np.ascontiguousarray(y.reshape(n, hm).T), np.array(desc)
+            print(dtype, "c2r members adjacent", n, desc, flush=True)
+    np.savez_compressed(os.path.join(HERE, f"{dtype}_c2r_reference.npz"), **out)
+
+
 def make_f32(kdir):
     kern = neon_a64.Kernels([os.path.join(kdir, s) for s in F32_SOURCES])
     out = {}
@@ -250,7 +286,7 @@ def make_real(kdir):
 
 def main():
     kdir = os.path.join(sys.argv[1], "src", "providers", "aot", "asm", "neon")
-    which = sys.argv[2:] or ["q15", "q7", "f32", "real", "q15r", "q7r"]
+    which = sys.argv[2:] or ["q15", "q7", "f32", "real", "q15r", "q7r", "q15cr", "q7cr"]
     if "q15" in which:
         make_fixed(kdir, "q15", 16)
     if "q7" in which:
@@ -263,6 +299,10 @@ def main():
         make_fixed_real(kdir, "q15", 16)
     if "q7r" in which:
         make_fixed_real(kdir, "q7", 8)
+    if "q15cr" in which:
+        make_fixed_c2r(kdir, "q15", 16)
+    if "q7cr" in which:
+        make_fixed_c2r(kdir, "q7", 8)
 
 
 if __name__ == "__main__":
