@@ -741,6 +741,317 @@ cudaError_t launch_fixed_r2c(int bits, int n, const FixedLaunch& L, cudaStream_t
   return bits == 16 ? launch_fx_r2c<16>(n, L, st) : launch_fx_r2c<8>(n, L, st);
 }
 
+// ---- C2R (backward): the reference's real-output plans ----
+// The C2R plan runs the decomposition backward with decimation in frequency
+// (planner/strategies/cooley_tukey.hpp:250-323, 498-580): a radix-16 DIF
+// level over rows j = 0..m/2 of the Hermitian input (row j takes
+// X[j + m i], the ones past the stored half as conjugates of
+// X[m (16 - i) - j]; a backward 16-point codelet; outputs k >= 1 of rows
+// j >= 1 times W_N^{jk}), then per column a real-output codelet of length
+// m (n <= 256) or a second such level over m/16 rows and real-output
+// codelets of length m/16 on 256 lanes (n >= 512).  Inputs are pre-shifted
+// by log2 of the codelet length, then conjugated as products by
+// (1 - 2^-(B-1), -1).  The real-output codelets of lengths 2 and 4 are the
+// backward codelet's real parts; those of 8 and 16 round their constant
+// products in their own places (cr_real8, cr_real16).  The operands here
+// reach the full lane range, so every add saturates and every MAC wraps at
+// 2B bits, as the reference's sqadd / smlal lanes do.
+
+template <int B>
+__device__ __forceinline__ int cr_add(int a, int b) { return fx_sat<B>(a + b); }
+template <int B>
+__device__ __forceinline__ int cr_sub(int a, int b) { return fx_sat<B>(a - b); }
+// a times the constant k, one rounding, saturated
+template <int B>
+__device__ __forceinline__ int cr_rdm(int a, int k) { return fx_sat<B>((a * k + (1 << (B - 2))) >> (B - 1)); }
+// two products accumulated in a 2B-bit lane (wrapping), one rounding narrow
+template <int B>
+__device__ __forceinline__ int cr_mac2(int a, int ka, int b, int kb) {
+  const unsigned u = unsigned(a) * unsigned(ka) + unsigned(b) * unsigned(kb);
+  const int64_t acc = B == 16 ? int64_t(int(u)) : int64_t(short(u & 0xffffu));
+  return fx_sat<B>(int((acc + (1 << (B - 2))) >> (B - 1)));
+}
+// pre-shifted input, conjugated by the constant products when asked
+template <int B>
+__device__ __forceinline__ qc cr_in(qc v, int s, bool conj) {
+  const qc a = s ? qc{rshr(v.re, s), rshr(v.im, s)} : v;
+  return conj ? qc{cr_rdm<B>(a.re, Fx<B>::HI), cr_rdm<B>(a.im, Fx<B>::LO)} : a;
+}
+
+// real-output codelet of length 8 on the extended, pre-shifted inputs A
+template <int B>
+__device__ __forceinline__ void cr_real8(const qc* A, int* x) {
+  constexpr int C8 = Fx<B>::C8;
+  const int s04 = cr_add<B>(A[0].re, A[4].re), d04 = cr_sub<B>(A[0].re, A[4].re);
+  const int s26 = cr_add<B>(A[2].re, A[6].re), e26 = cr_sub<B>(A[2].im, A[6].im);
+  const qc p15 = {cr_sub<B>(A[1].re, A[5].re), cr_sub<B>(A[1].im, A[5].im)};
+  const qc p37 = {cr_sub<B>(A[3].re, A[7].re), cr_sub<B>(A[3].im, A[7].im)};
+  const int qr = cr_add<B>(cr_add<B>(A[1].re, A[5].re), cr_add<B>(A[3].re, A[7].re));
+  const int qi = cr_sub<B>(cr_add<B>(A[1].im, A[5].im), cr_add<B>(A[3].im, A[7].im));
+  const int u = cr_rdm<B>(cr_sub<B>(p15.re, p37.re), C8);
+  const int v = cr_rdm<B>(cr_add<B>(p15.im, p37.im), C8);
+  const int e = cr_add<B>(s04, s26), g = cr_sub<B>(s04, s26);
+  const int a = cr_add<B>(d04, u), b = cr_sub<B>(fx_sat<B>(-e26), v);
+  const int c = cr_sub<B>(d04, u), d = cr_sub<B>(v, e26);
+  x[0] = cr_add<B>(e, qr);
+  x[4] = cr_sub<B>(e, qr);
+  x[2] = cr_sub<B>(g, qi);
+  x[6] = cr_add<B>(g, qi);
+  x[1] = cr_add<B>(a, b);
+  x[7] = cr_sub<B>(a, b);
+  x[3] = cr_sub<B>(c, d);
+  x[5] = cr_add<B>(c, d);
+}
+
+// real-output codelet of length 16 on the extended, pre-shifted inputs A
+template <int B>
+__device__ __forceinline__ void cr_real16(const qc* A, int* x) {
+  constexpr int C8 = Fx<B>::C8, C16 = Fx<B>::C16, S16 = Fx<B>::S16, HI = Fx<B>::HI, LO = Fx<B>::LO;
+  auto ad = [](int a, int b) { return cr_add<B>(a, b); };
+  auto sb = [](int a, int b) { return cr_sub<B>(a, b); };
+  auto rd = [](int a, int k) { return cr_rdm<B>(a, k); };
+  auto mc = [](int a, int ka, int b, int kb) { return cr_mac2<B>(a, ka, b, kb); };
+  // even half: inputs 0, 2, ..., 14
+  const int s08 = ad(A[0].re, A[8].re), d08 = sb(A[0].re, A[8].re);
+  const int s4c = ad(A[4].re, A[12].re), d4c = sb(A[4].im, A[12].im);
+  const int ev = ad(s08, s4c), ew = sb(s08, s4c);
+  const int s2a6e = ad(ad(A[2].re, A[10].re), ad(A[6].re, A[14].re));
+  const int r2a = sb(A[2].re, A[10].re), i2a = sb(A[2].im, A[10].im);
+  const int r6e = sb(A[6].re, A[14].re), i6e = sb(A[6].im, A[14].im);
+  const int i26 = sb(ad(A[2].im, A[10].im), ad(A[6].im, A[14].im));
+  const int e0 = ad(ev, s2a6e), e4 = sb(ev, s2a6e);
+  const int f1 = sb(d08, d4c), f3 = ad(d08, d4c);
+  const int f2 = sb(ew, i26), f6 = ad(ew, i26);
+  // odd half: inputs 1, 3, ..., 15
+  const int s19 = ad(A[1].re, A[9].re), s5d = ad(A[5].re, A[13].re);
+  const int s3b = ad(A[3].re, A[11].re), s7f = ad(A[7].re, A[15].re);
+  const int o0 = ad(ad(s19, s5d), ad(s3b, s7f));
+  const int i3b = sb(A[3].im, A[11].im), r7f = rd(sb(A[7].re, A[15].re), HI);
+  const int r3b = sb(A[3].re, A[11].re), i7f = rd(sb(A[7].im, A[15].im), LO);
+  const int i19 = sb(A[1].im, A[9].im), r5d = rd(sb(A[5].re, A[13].re), HI);
+  const int r19 = sb(A[1].re, A[9].re), i5d = rd(sb(A[5].im, A[13].im), LO);
+  const int p3 = ad(i3b, r7f), q3 = ad(r3b, i7f), p1 = ad(i19, r5d), q1 = ad(r19, i5d);
+  const int m3 = sb(i3b, r7f), n3 = sb(r3b, i7f), m1 = sb(i19, r5d), n1 = sb(r19, i5d);
+  const int j3b = ad(A[3].im, A[11].im), j7f = ad(A[7].im, A[15].im), j37 = sb(j3b, j7f);
+  const int k37 = sb(s3b, s7f);
+  const int j19 = ad(A[1].im, A[9].im), j5d = ad(A[5].im, A[13].im), j15 = sb(j19, j5d);
+  const int k15 = sb(s19, s5d);
+  const int o4 = sb(ad(j19, j5d), ad(j3b, j7f));
+  // rotations
+  const int w1 = rd(sb(mc(i6e, -C8, rd(r6e, -C8), HI), mc(i2a, C8, rd(r2a, C8), LO)), LO);
+  const int w3 = ad(mc(r2a, C8, rd(i2a, C8), HI), mc(r6e, -C8, rd(i6e, -C8), LO));
+  const int z2 = rd(sb(mc(j37, -C8, rd(k37, -C8), HI), mc(j15, C8, rd(k15, C8), LO)), LO);
+  const int z6 = ad(mc(k15, C8, rd(j15, C8), HI), mc(k37, -C8, rd(j37, -C8), LO));
+  const int z1 = rd(sb(mc(p3, -C16, q3, S16), mc(p1, S16, q1, -C16)), LO);
+  const int z3 = rd(sb(mc(m3, S16, n3, -C16), mc(m1, C16, n1, -S16)), LO);
+  const int z5 = ad(mc(q1, S16, p1, C16), mc(q3, -C16, p3, -S16));
+  const int z7 = ad(mc(n1, C16, m1, S16), mc(n3, S16, m3, C16));
+  const int g1 = sb(f1, w1), g5 = ad(f1, w1), g3 = sb(f3, w3), g7 = ad(f3, w3);
+  x[0] = ad(e0, o0);
+  x[8] = sb(e0, o0);
+  x[4] = sb(e4, o4);
+  x[12] = ad(e4, o4);
+  x[2] = sb(f2, z2);
+  x[10] = ad(f2, z2);
+  x[6] = sb(f6, z6);
+  x[14] = ad(f6, z6);
+  x[1] = sb(g1, z1);
+  x[9] = ad(g1, z1);
+  x[3] = sb(g3, z3);
+  x[11] = ad(g3, z3);
+  x[5] = sb(g5, z5);
+  x[13] = ad(g5, z5);
+  x[7] = sb(g7, z7);
+  x[15] = ad(g7, z7);
+}
+
+// real-output codelet of length R over the stored half get(e), e = 0..R/2
+template <int R, int B, class Get>
+__device__ __forceinline__ void cr_real_out(Get get, int* x) {
+  constexpr int S = ilog2_c(R);
+  qc A[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) A[i] = i <= R / 2 ? cr_in<B>(get(i), S, false) : cr_in<B>(get(R - i), S, true);
+  if constexpr (R == 8) {
+    cr_real8<B>(A, x);
+  } else if constexpr (R == 16) {
+    cr_real16<B>(A, x);
+  } else {
+    qc y[R];
+    q_dft<R, B>(A, y);
+#pragma unroll
+    for (int k = 0; k < R; ++k) x[k] = fx_sat<B>(y[(R - k) % R].re);  // backward: forward output R - k
+  }
+}
+
+// row j of a radix-16 DIF level over ROWS_ rows of a Hermitian sequence of
+// length 16 rows (stored half get(e), e = 0..8 rows): 16 outputs, those
+// k >= 1 of rows j >= 1 times the row's twiddle tw[15 (j - 1) + k - 1]
+template <int B, class Get>
+__device__ __forceinline__ void cr_dif_row(Get get, int rows, int j, const short4* tw, qc* out) {
+  qc a[16], t[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const bool direct = j == 0 ? i <= 8 : i <= 7;
+    a[i] = cr_in<B>(get(direct ? j + rows * i : rows * (16 - i) - j), 4, !direct);
+  }
+  q_dft<16, B>(a, t);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    const qc v = {fx_sat<B>(t[(16 - k) & 15].re), fx_sat<B>(t[(16 - k) & 15].im)};  // backward output k
+    if (j > 0 && k > 0) {
+      const short4 w = __ldg(tw + 15 * (j - 1) + (k - 1));  // (c, s, cvt(-s), c)
+      out[k] = {cr_mac2<B>(v.re, w.x, v.im, w.z), cr_mac2<B>(v.re, w.y, v.im, w.w)};
+    } else {
+      out[k] = v;
+    }
+  }
+}
+
+// n <= 16: one thread per member
+template <int N, int B>
+__global__ void __launch_bounds__(256) fx_c2r_small_kernel(const FixedLaunch L) {
+  using W = typename Fx<B>::W;
+  griddep_wait();  // launched programmatically (launch_pdl.cuh)
+  griddep_launch_dependents();
+  const int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b >= L.howmany) return;
+  const W* X = static_cast<const W*>(L.in) + b * L.idist;
+  FxS<B>* y = static_cast<FxS<B>*>(L.out) + b * L.odist;
+  qc h[N / 2 + 1];
+#pragma unroll
+  for (int k = 0; k <= N / 2; ++k) h[k] = unpack(X[k * L.istride]);
+  int x[N];
+  cr_real_out<N, B>([&](int e) { return h[e]; }, x);
+#pragma unroll
+  for (int t = 0; t < N; ++t) y[t * L.ostride] = FxS<B>(x[t]);
+}
+
+// shared-memory layout of the C2R kernels: the members' stored halves
+// (H words each), the first level's rows 0..m/2 (16 words each), [the
+// second level's rows 0..m'/2 (256 words each)], the output reals
+template <int B>
+__host__ __device__ constexpr int cr_align16(int bytes) { return (bytes + 15) / 16 * 16; }
+template <int N, int B>
+struct CrSmem {
+  static constexpr int H = N / 2 + 1, M = N / 16, ROWS = M / 2 + 1;
+  static constexpr int M2 = N > 256 ? N / 256 : 0, ROWS2 = M2 / 2 + 1;
+  static constexpr int G = N > 256 ? 1 : 16;  // members per CTA
+  static constexpr int WB = int(sizeof(typename Fx<B>::W));
+  static constexpr int X_OFF = 0;
+  static constexpr int B_OFF = cr_align16<B>(X_OFF + G * H * WB);
+  static constexpr int C_OFF = cr_align16<B>(B_OFF + G * ROWS * 16 * WB);
+  static constexpr int O_OFF = cr_align16<B>(C_OFF + (M2 ? ROWS2 * 256 * WB : 0));
+  static constexpr int BYTES = cr_align16<B>(O_OFF + G * N * int(sizeof(FxS<B>)));
+};
+
+// n = 16 m (m = 2..16, 16 members per CTA) or n = 256 m' (m' = 2..16, one
+// member per CTA); 256 threads
+template <int N, int B>
+__global__ void __launch_bounds__(256) fx_c2r_kernel(const FixedLaunch L) {
+  using W = typename Fx<B>::W;
+  using Sm = CrSmem<N, B>;
+  constexpr int H = Sm::H, M = Sm::M, ROWS = Sm::ROWS, M2 = Sm::M2, ROWS2 = Sm::ROWS2, G = Sm::G;
+  griddep_wait();  // launched programmatically (launch_pdl.cuh)
+  griddep_launch_dependents();
+  extern __shared__ __align__(16) unsigned char fsm[];
+  W* xs = reinterpret_cast<W*>(fsm + Sm::X_OFF);
+  W* bs = reinterpret_cast<W*>(fsm + Sm::B_OFF);
+  W* cs = reinterpret_cast<W*>(fsm + Sm::C_OFF);
+  FxS<B>* os = reinterpret_cast<FxS<B>*>(fsm + Sm::O_OFF);
+  const int64_t b0 = int64_t(blockIdx.x) * G;
+  const int64_t left = L.howmany - b0;
+  const int cnt = left < G ? int(left) : G;
+  const W* X = static_cast<const W*>(L.in);
+  for (int f = threadIdx.x; f < cnt * H; f += blockDim.x) {
+    const int g = f / H, e = f - g * H;
+    xs[f] = X[(b0 + g) * L.idist + int64_t(e) * L.istride];
+  }
+  __syncthreads();
+  // first level: rows j = 0..m/2 of each member
+  for (int task = threadIdx.x; task < cnt * ROWS; task += blockDim.x) {
+    const int g = task / ROWS, j = task - g * ROWS;
+    const W* src = xs + g * H;
+    qc r[16];
+    cr_dif_row<B>([&](int e) { return unpack(src[e]); }, M, j, L.tw, r);
+    W* dst = bs + (g * ROWS + j) * 16;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) dst[k] = pack<B>(r[k]);
+  }
+  __syncthreads();
+  if constexpr (M2 == 0) {
+    // real-output codelets of length m down the 16 columns
+    for (int task = threadIdx.x; task < cnt * 16; task += blockDim.x) {
+      const int g = task >> 4, k = task & 15;
+      const W* col = bs + g * ROWS * 16 + k;
+      int x[M];
+      cr_real_out<M, B>([&](int e) { return unpack(col[16 * e]); }, x);
+#pragma unroll
+      for (int t = 0; t < M; ++t) os[g * N + k + 16 * t] = FxS<B>(x[t]);
+    }
+  } else {
+    // second level: rows i = 0..m'/2 of each column's length-m sequence
+    for (int task = threadIdx.x; task < 16 * ROWS2; task += blockDim.x) {
+      const int k = task / ROWS2, i = task - k * ROWS2;
+      qc r[16];
+      cr_dif_row<B>([&](int e) { return unpack(bs[16 * e + k]); }, M2, i, L.tw2, r);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) cs[256 * i + 16 * q + k] = pack<B>(r[q]);
+    }
+    __syncthreads();
+    // real-output codelets of length m' on the 256 lanes
+    for (int l = threadIdx.x; l < 256; l += blockDim.x) {
+      int x[M2];
+      cr_real_out<M2, B>([&](int e) { return unpack(cs[256 * e + l]); }, x);
+#pragma unroll
+      for (int t = 0; t < M2; ++t) os[l + 256 * t] = FxS<B>(x[t]);
+    }
+  }
+  __syncthreads();
+  FxS<B>* y = static_cast<FxS<B>*>(L.out);
+  for (int f = threadIdx.x; f < cnt * N; f += blockDim.x) {
+    const int g = f / N, t = f - g * N;
+    y[(b0 + g) * L.odist + int64_t(t) * L.ostride] = os[f];
+  }
+}
+
+template <int N, int B>
+static cudaError_t run_fx_c2r(const FixedLaunch& L, cudaStream_t st) {
+  if constexpr (N <= 16) {
+    const int64_t blocks = (L.howmany + 255) / 256;
+    return launch_pdl(fx_c2r_small_kernel<N, B>, dim3(unsigned(blocks)), dim3(256), 0, st, L);
+  } else {
+    using Sm = CrSmem<N, B>;
+    static_assert(Sm::BYTES <= 48 * 1024, "default dynamic shared-memory limit");
+    const int64_t blocks = (L.howmany + Sm::G - 1) / Sm::G;
+    return launch_pdl(fx_c2r_kernel<N, B>, dim3(unsigned(blocks)), dim3(256), size_t(Sm::BYTES), st, L);
+  }
+}
+
+template <int B>
+static cudaError_t launch_fx_c2r(int n, const FixedLaunch& L, cudaStream_t st) {
+  switch (n) {
+    case 2: return run_fx_c2r<2, B>(L, st);
+    case 4: return run_fx_c2r<4, B>(L, st);
+    case 8: return run_fx_c2r<8, B>(L, st);
+    case 16: return run_fx_c2r<16, B>(L, st);
+    case 32: return run_fx_c2r<32, B>(L, st);
+    case 64: return run_fx_c2r<64, B>(L, st);
+    case 128: return run_fx_c2r<128, B>(L, st);
+    case 256: return run_fx_c2r<256, B>(L, st);
+    case 512: return run_fx_c2r<512, B>(L, st);
+    case 1024: return run_fx_c2r<1024, B>(L, st);
+    case 2048: return run_fx_c2r<2048, B>(L, st);
+    case 4096: return run_fx_c2r<4096, B>(L, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_fixed_c2r(int bits, int n, const FixedLaunch& L, cudaStream_t st) {
+  if (L.howmany > 0x7fffffffLL && n > 256) return cudaErrorInvalidValue;  // one CTA per member
+  return bits == 16 ? launch_fx_c2r<16>(n, L, st) : launch_fx_c2r<8>(n, L, st);
+}
+
 template <int B>
 static cudaError_t launch_fx(int n, int dir, const FixedLaunch& L, cudaStream_t st) {
 #define PLFFT_B200_FX(NV) \

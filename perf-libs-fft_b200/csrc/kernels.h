@@ -322,6 +322,10 @@ cudaError_t launch_fixed(int bits, int n, int dir, const FixedLaunch& L, cudaStr
 // or int8 lanes; istride / idist in reals), output bins 0..n/2 (packed
 // complex; ostride / odist in complex elements); tw / tw2 as for the C2C
 cudaError_t launch_fixed_r2c(int bits, int n, const FixedLaunch& L, cudaStream_t st);
+// fixed-point C2R (backward), power-of-two n in [2, 4096]: input bins 0..n/2
+// (packed complex; istride / idist in complex elements), output reals
+// (ostride / odist in reals); tw / tw2: the backward tables
+cudaError_t launch_fixed_c2r(int bits, int n, const FixedLaunch& L, cudaStream_t st);
 
 // Split-BF16 tensor-core pass (split_bf16.cu): same addressing as a
 // four-step pass, on-chip length nl in {256, 4096} as radix-16 DFT-matrix

@@ -178,7 +178,7 @@ std::unique_ptr<Node> autotune_c2c(const ConfigData& c, const Layout& lay, std::
 std::unique_ptr<Node> make_fp64_node(int kind, int64_t n, const Layout& lay, int dir, double scale,
                                      std::string* why);
 
-// Fixed-point C2C (kind 0) or R2C (kind 1) node (plan_fixed.cpp), bits 16
+// Fixed-point C2C (kind 0), R2C (kind 1) or C2R (kind 2) node (plan_fixed.cpp), bits 16
 // (Q0.15) or 8 (Q0.7); nullptr (with why) if unsupported.
 std::unique_ptr<Node> make_fixed_node(int bits, int64_t n, const Layout& lay, int dir, std::string* why,
                                       int kind = 0);

@@ -1,12 +1,13 @@
-// Fixed-point C2C plan node, Q0.15 and Q0.7 (kernels in fixed_point.cu).
+// Fixed-point plan node, Q0.15 and Q0.7 (kernels in fixed_point.cu).
 //
 // The reference plans fixed-point C2C / R2C / C2R and rejects fixed-point
 // R2R (src/plfft.cpp:248-261); every fixed-point transform is scaled by
-// 1/n (docs/plfft.md:128-130).  The device path covers C2C and R2C of
+// 1/n (docs/plfft.md:128-130).  The device path covers C2C, R2C and C2R of
 // power-of-two n <= 4096 with the reference's ESTIMATE decomposition
 // (radix-16 cooley_tukey_ab, over a radix-16 cooley_tukey_ac for n > 256;
-// the R2C levels with mirrored rows); C2R and other fixed-point
-// configurations fail plan creation with a reason.
+// the R2C levels with mirrored rows, the C2R ones decimating in frequency
+// over the Hermitian half); other fixed-point configurations fail plan
+// creation with a reason.
 #include <cmath>
 
 #include "plan.hpp"
@@ -38,28 +39,32 @@ static std::vector<short4> radix16_twiddles(int64_t n1, int dir, int bits) {
 
 struct FixedNode : Node {
   int bits = 16, n = 0, dir = -1;
-  bool r2c = false;
+  int kind = 0;  // 0 C2C, 1 R2C, 2 C2R
   FixedLaunch base{};
   DevBuf tw, tw2;
   cudaError_t run(const void* in, void* out, void*, cudaStream_t st) const override {
     FixedLaunch L = base;
     L.in = in;
     L.out = out;
-    return r2c ? launch_fixed_r2c(bits, n, L, st) : launch_fixed(bits, n, dir, L, st);
+    if (kind == 1) return launch_fixed_r2c(bits, n, L, st);
+    if (kind == 2) return launch_fixed_c2r(bits, n, L, st);
+    return launch_fixed(bits, n, dir, L, st);
   }
   std::string describe() const override {
     const char* shape = n <= 16 ? " one codelet" : (n <= 256 ? " 16-column x twiddled-row codelets"
                                                               : " 256-column codelets, radix-16 ac and ab levels");
-    return std::string(r2c ? "(r2c-" : "(c2c-") + (bits == 16 ? "q15" : "q7") + " n=" + std::to_string(n) + shape +
-           (r2c ? ", mirrored rows" : "") + ")";
+    static const char* names[] = {"(c2c-", "(r2c-", "(c2r-"};
+    static const char* notes[] = {"", ", mirrored rows", ", DIF rows of the Hermitian half"};
+    return std::string(names[kind]) + (bits == 16 ? "q15" : "q7") + " n=" + std::to_string(n) + shape + notes[kind] +
+           ")";
   }
 };
 
 // kind: 0 C2C (dir as given), 1 R2C (forward; input reals, output bins
-// 0..n/2)
+// 0..n/2), 2 C2R (backward; input bins 0..n/2, output reals)
 std::unique_ptr<Node> make_fixed_node(int bits, int64_t n, const Layout& lay, int dir, std::string* why, int kind) {
-  if (!fixed_supported(n) || (kind == 1 && n < 2)) {
-    if (why) *why = "fixed-point C2C / R2C on the device cover power-of-two n <= 4096 (R2C: n >= 2)";
+  if (!fixed_supported(n) || (kind != 0 && n < 2)) {
+    if (why) *why = "fixed-point transforms on the device cover power-of-two n <= 4096 (R2C / C2R: n >= 2)";
     return nullptr;
   }
   if (n > 256 && lay.howmany > 0x7fffffffLL) {
@@ -69,8 +74,8 @@ std::unique_ptr<Node> make_fixed_node(int bits, int64_t n, const Layout& lay, in
   auto node = std::make_unique<FixedNode>();
   node->bits = bits;
   node->n = int(n);
-  node->r2c = kind == 1;
-  node->dir = kind == 1 ? -1 : dir;
+  node->kind = kind;
+  node->dir = kind == 1 ? -1 : (kind == 2 ? 1 : dir);
   dir = node->dir;
   node->base.howmany = lay.howmany;
   node->base.istride = lay.istride;

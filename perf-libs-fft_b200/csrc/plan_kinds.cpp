@@ -111,14 +111,14 @@ static std::unique_ptr<Node> make_root(const ConfigData& c, const Layout& lay, b
       root = make_half_node(c, lay, why);
     }
   } else if ((c.data_type == PLFFT_DATA_TYPE_Q15 || c.data_type == PLFFT_DATA_TYPE_Q7) &&
-             (c.kind == TKind::C2C || c.kind == TKind::R2C)) {
+             (c.kind == TKind::C2C || c.kind == TKind::R2C || c.kind == TKind::C2R)) {
     if (c.scale != 1.0) {
       if (why) *why = "fixed-point transforms are scaled by 1/n and take no extra scale";
     } else if (c.precision != 0) {
       if (why) *why = "the split-BF16 precision mode takes FP32 data";
     } else {
       root = make_fixed_node(c.data_type == PLFFT_DATA_TYPE_Q15 ? 16 : 8, c.n, lay, c.payload, why,
-                             c.kind == TKind::R2C ? 1 : 0);
+                             c.kind == TKind::R2C ? 1 : (c.kind == TKind::C2R ? 2 : 0));
     }
   } else if ((c.data_type == PLFFT_DATA_TYPE_Q15 || c.data_type == PLFFT_DATA_TYPE_Q7) &&
              c.kind == TKind::R2R) {
