@@ -1,6 +1,6 @@
 /*
- * Bit-exact CPU restatement of the reference's fixed-point C2C and R2C
- * paths, Q0.15 and Q0.7 -- TEST INFRASTRUCTURE ONLY (same rules as oracle.c: only tests/
+ * Bit-exact CPU restatement of the reference's fixed-point C2C, R2C and
+ * C2R paths, Q0.15 and Q0.7 -- TEST INFRASTRUCTURE ONLY (same rules as oracle.c: only tests/
  * and the CPU-baseline leg of bench.py load it, to check results).
  *
  * What is restated (arm/perf-libs-fft), for lanes of B = 16 or 8 bits:
@@ -50,7 +50,9 @@
  * plans (executed from their source text by tests/golden/neon_a64.py);
  * tests/test_q15.py and tests/test_q7.py require this file to match them
  * bit for bit; q15_r2c_reference.npz and q7_r2c_reference.npz pin the R2C
- * (fixed_r2c below) the same way (tests/test_fixed_r2c.py).
+ * (fixed_r2c below) the same way (tests/test_fixed_r2c.py), and
+ * q15_c2r_reference.npz and q7_c2r_reference.npz the C2R (fixed_c2r,
+ * tests/test_fixed_c2r.py).
  *
  * Data: interleaved (re, im) of int16 (Q0.15) or int8 (Q0.7), members
  * idist/odist complex elements apart, unit element stride (R2C: real
